@@ -1,0 +1,343 @@
+"""diana_tucker_b200 -- DIANA-Tucker's HOOI-ALS hot path on B200 (sm_100a).
+
+Python host layer over the C ABI of ``libdt_cuda.so`` (include/dt_cuda.h).
+Every computation runs in the CUDA library; this module only moves buffers:
+numpy arrays are passed as host pointers (the library stages them), torch
+CUDA tensors are passed as device pointers on torch's current stream.
+
+The C++ drop-in for the reference's own API (``Tensor<Ty>``, ``SpTensor<Ty>``,
+``Function::ttm``, ``Algorithm::Tucker::HOOI_ALS`` ...) lives in
+``cpp/include/diana``.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import (DT_INIT_GIVEN, DT_INIT_HOSVD, DT_INIT_RANDN_LIBC, DT_PREC_BF16,
+                   DT_PREC_BF16X2, DT_PREC_FP64, DTError, HooiOpts, HooiReport)
+
+__all__ = ["Context", "SpTensor", "DTError", "DT_PREC_FP64", "DT_PREC_BF16", "DT_PREC_BF16X2",
+           "DT_INIT_RANDN_LIBC", "DT_INIT_HOSVD", "DT_INIT_GIVEN"]
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _shape_arr(shape):
+    return np.ascontiguousarray(np.asarray(shape, dtype=np.int64))
+
+
+def _i64p(a: np.ndarray):
+    return a.ctypes.data_as(_lib.c_i64p)
+
+
+class _Buf:
+    """A caller buffer as (pointer, keep-alive owner)."""
+
+    def __init__(self, x, dtype=np.float64, fortran=True, writable=False):
+        self.torch = _is_torch(x)
+        if self.torch:
+            import torch
+            tdt = torch.float64 if dtype == np.float64 else torch.float32
+            if x.dtype != tdt:
+                raise TypeError(f"expected {tdt}, got {x.dtype}")
+            self.obj = x
+            self.ptr = ctypes.c_void_p(x.data_ptr())
+        else:
+            a = np.asarray(x, dtype=dtype)
+            a = np.asfortranarray(a) if fortran else np.ascontiguousarray(a)
+            if writable and a is not x:
+                a = a.copy(order="F" if fortran else "C")
+            self.obj = a
+            self.ptr = ctypes.c_void_p(a.ctypes.data)
+
+
+def _alloc_like(ref_is_torch, shape, dtype=np.float64, device=None):
+    if ref_is_torch:
+        import torch
+        # Column-major storage: allocate the reversed shape C-contiguous and
+        # expose it transposed, so data_ptr() holds the col-major layout.
+        t = torch.empty(tuple(reversed(shape)), dtype=torch.float64, device=device)
+        return t.permute(*reversed(range(len(shape)))) if len(shape) > 1 else t
+    return np.zeros(shape, dtype=dtype, order="F")
+
+
+class Context:
+    """A dt_ctx bound to one GPU (dt_ctx_create)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        h = ctypes.c_void_p()
+        _lib.check(self.lib.dt_ctx_create(device, ctypes.byref(h)))
+        self.h = h
+        self.device = device
+        self._torch_stream = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dt_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- stream plumbing --------------------------------------------------
+    def _bind(self, *objs):
+        """Runs on torch's current stream when torch tensors are involved."""
+        if any(_is_torch(o) for o in objs):
+            import torch
+            s = torch.cuda.current_stream(self.device).cuda_stream
+            if s != self._torch_stream:
+                _lib.check(self.lib.dt_ctx_set_stream(self.h, ctypes.c_void_p(s)))
+                self._torch_stream = s
+        elif self._torch_stream is not None:
+            _lib.check(self.lib.dt_ctx_set_stream(self.h, None))
+            self._torch_stream = None
+
+    def synchronize(self):
+        _lib.check(self.lib.dt_ctx_synchronize(self.h))
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.dt_ctx_kernel_launches(self.h))
+
+    # -- operators -----------------------------------------------------------
+    def ttm(self, X, M, n: int):
+        """Y = X x_n M (Function::ttm)."""
+        self._bind(X, M)
+        shape = list(X.shape)
+        J = int(M.shape[0])
+        xb, mb = _Buf(X), _Buf(M)
+        out_shape = shape.copy()
+        out_shape[n] = J
+        Y = _alloc_like(xb.torch, out_shape, device=getattr(X, "device", None))
+        yb = _Buf(Y)
+        s = _shape_arr(shape)
+        _lib.check(self.lib.dt_ttm_f64(self.h, xb.ptr, len(shape), _i64p(s), n, mb.ptr,
+                                       J, yb.ptr))
+        return Y
+
+    def gram(self, X, n: int):
+        self._bind(X)
+        xb = _Buf(X)
+        G = _alloc_like(xb.torch, [X.shape[n], X.shape[n]], device=getattr(X, "device", None))
+        gb = _Buf(G)
+        s = _shape_arr(X.shape)
+        _lib.check(self.lib.dt_gram_f64(self.h, xb.ptr, X.ndim if not xb.torch else X.dim(),
+                                        _i64p(s), n, gb.ptr))
+        return G
+
+    def ttt_except(self, A, B, n: int):
+        self._bind(A, B)
+        ab, bb = _Buf(A), _Buf(B)
+        nd = len(A.shape)
+        C = _alloc_like(ab.torch, [A.shape[n], B.shape[n]], device=getattr(A, "device", None))
+        cb = _Buf(C)
+        sa, sb = _shape_arr(A.shape), _shape_arr(B.shape)
+        _lib.check(self.lib.dt_ttt_except_f64(self.h, ab.ptr, _i64p(sa), bb.ptr, _i64p(sb),
+                                              nd, n, cb.ptr))
+        return C
+
+    def fnorm(self, X) -> float:
+        self._bind(X)
+        xb = _Buf(X)
+        out = ctypes.c_double()
+        n = int(np.prod(X.shape))
+        _lib.check(self.lib.dt_fnorm_f64(self.h, xb.ptr, n, ctypes.byref(out)))
+        return out.value
+
+    def matmul(self, A, B, transA=False, transB=False):
+        """C = op(A) op(B) (Operator::matmulNN/NT/TN)."""
+        self._bind(A, B)
+        A = np.asfortranarray(A, dtype=np.float64)
+        B = np.asfortranarray(B, dtype=np.float64)
+        m = A.shape[1] if transA else A.shape[0]
+        k = A.shape[0] if transA else A.shape[1]
+        n = B.shape[0] if transB else B.shape[1]
+        C = np.zeros((m, n), order="F")
+        _lib.check(self.lib.dt_matmul_f64(self.h, int(transA), int(transB), m, n, k,
+                                          A.ctypes.data, B.ctypes.data, C.ctypes.data))
+        return C
+
+    def reduced_qr(self, A):
+        self._bind(A)
+        A = np.asfortranarray(A, dtype=np.float64)
+        m, n = A.shape
+        Q = np.zeros((m, n), order="F")
+        R = np.zeros((n, n), order="F")
+        _lib.check(self.lib.dt_reduced_qr_f64(self.h, A.ctypes.data, m, n, Q.ctypes.data,
+                                              R.ctypes.data))
+        return Q, R
+
+    def inverse(self, A):
+        self._bind(A)
+        A = np.asfortranarray(A, dtype=np.float64)
+        out = np.zeros_like(A, order="F")
+        _lib.check(self.lib.dt_inverse_f64(self.h, A.ctypes.data, A.shape[0], out.ctypes.data))
+        return out
+
+    def orth2(self, A):
+        """Row orthonormalisation of the R x I matrix A (Operator::orth2)."""
+        self._bind(A)
+        a = np.asfortranarray(np.array(A, dtype=np.float64, copy=True))
+        _lib.check(self.lib.dt_orth2_f64(self.h, a.ctypes.data, a.shape[0], a.shape[1]))
+        return a
+
+    def als(self, Y, n, L0, iters=5):
+        self._bind(Y)
+        yb = _Buf(Y)
+        L0 = np.asfortranarray(L0, dtype=np.float64)
+        Q = np.zeros_like(L0, order="F")
+        s = _shape_arr(Y.shape)
+        _lib.check(self.lib.dt_als_f64(self.h, yb.ptr, len(Y.shape), _i64p(s), n,
+                                       L0.ctypes.data, L0.shape[1], iters, Q.ctypes.data))
+        return Q
+
+    # -- dense HOOI ----------------------------------------------------------
+    def hooi_dense(self, X, ranks, *, init="randn", seed=1, U0=None, max_sweeps=5, tol=0.0,
+                   inner_iters=5, precision=DT_PREC_FP64, refine_sweeps=0, verbose=False,
+                   want_factors=True, want_core=True):
+        """Algorithm::Tucker::HOOI_ALS.  X: numpy or torch (float64/float32),
+        column-major.  Returns (G, U, report-dict)."""
+        self._bind(X)
+        is_torch = _is_torch(X)
+        if is_torch:
+            import torch
+            dtype = _lib.DT_F64 if X.dtype == torch.float64 else _lib.DT_F32
+            xptr = ctypes.c_void_p(X.data_ptr())
+            shape = list(X.shape)
+        else:
+            X = np.asarray(X)
+            if X.dtype not in (np.float64, np.float32):
+                X = X.astype(np.float64)
+            X = np.asfortranarray(X)
+            dtype = _lib.DT_F64 if X.dtype == np.float64 else _lib.DT_F32
+            xptr = ctypes.c_void_p(X.ctypes.data)
+            shape = list(X.shape)
+        N = len(shape)
+        ranks = [int(r) for r in ranks]
+        opts = HooiOpts()
+        self.lib.dt_hooi_default_opts(ctypes.byref(opts))
+        opts.init = {"randn": DT_INIT_RANDN_LIBC, "hosvd": DT_INIT_HOSVD,
+                     "given": DT_INIT_GIVEN}[init if U0 is None else "given"]
+        opts.seed = seed
+        opts.max_sweeps = max_sweeps
+        opts.tol = tol
+        opts.inner_iters = inner_iters
+        opts.precision = precision
+        opts.refine_sweeps = refine_sweeps
+        opts.verbose = int(verbose)
+        G = np.zeros(ranks, order="F") if want_core else None
+        U = ([np.zeros((shape[n], ranks[n]), order="F") for n in range(N)]
+             if (want_factors or U0 is not None) else None)
+        if U0 is not None:
+            for n in range(N):
+                U[n][...] = np.asarray(U0[n], dtype=np.float64)
+        Uptr = (ctypes.c_void_p * N)(*[u.ctypes.data for u in U]) if U is not None else None
+        rep = HooiReport()
+        s, r = _shape_arr(shape), _shape_arr(ranks)
+        _lib.check(self.lib.dt_hooi_dense(self.h, xptr, dtype, N, _i64p(s), _i64p(r),
+                                          ctypes.byref(opts),
+                                          ctypes.c_void_p(G.ctypes.data) if G is not None else None,
+                                          Uptr, ctypes.byref(rep)))
+        return G, U, rep.as_dict()
+
+    # -- sparse ----------------------------------------------------------------
+    def sptensor(self, idx, vals, shape):
+        return SpTensor(self, idx, vals, shape)
+
+
+class SpTensor:
+    """Device-resident COO tensor with per-mode sorted copies (dt_sptensor)."""
+
+    def __init__(self, ctx: Context, idx, vals, shape):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        ctx._bind()
+        self.ndim = len(shape)
+        self.shape = [int(s) for s in shape]
+        idx = [np.ascontiguousarray(i, dtype=np.int64) for i in idx]
+        vals = np.ascontiguousarray(vals, dtype=np.float64)
+        self.nnz = int(vals.shape[0])
+        ptrs = (ctypes.c_void_p * self.ndim)(*[i.ctypes.data for i in idx])
+        s = _shape_arr(self.shape)
+        h = ctypes.c_void_p()
+        _lib.check(self.lib.dt_sptensor_create(ctx.h, self.nnz, self.ndim, ptrs,
+                                               vals.ctypes.data, _i64p(s), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.dt_sptensor_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _Ut(self, Ut):
+        arrs = [np.ascontiguousarray(u, dtype=np.float64) for u in Ut]
+        return arrs, (ctypes.c_void_p * self.ndim)(*[a.ctypes.data for a in arrs])
+
+    def fnorm(self) -> float:
+        out = ctypes.c_double()
+        _lib.check(self.lib.dt_sp_fnorm(self.ctx.h, self.h, ctypes.byref(out)))
+        return out.value
+
+    @staticmethod
+    def _kron_len(R, mode):
+        P = 1
+        for m, r in enumerate(R):
+            if m != mode:
+                P *= int(r)
+        return P
+
+    def ttmc_mTR(self, Ut, R, mode):
+        keep, ptrs = self._Ut(Ut)
+        r = _shape_arr(R)
+        L = np.zeros((self._kron_len(R, mode), int(R[mode])), order="F")
+        _lib.check(self.lib.dt_sp_ttmc_mTR(self.ctx.h, self.h, ptrs, _i64p(r), mode,
+                                           L.ctypes.data))
+        return L
+
+    def ttmc_mTL(self, Ut, R, mode, L):
+        keep, ptrs = self._Ut(Ut)
+        r = _shape_arr(R)
+        Lf = np.asfortranarray(L, dtype=np.float64)
+        out = np.zeros((self.shape[mode], int(R[mode])))
+        _lib.check(self.lib.dt_sp_ttmc_mTL(self.ctx.h, self.h, ptrs, _i64p(r), mode,
+                                           Lf.ctypes.data, out.ctypes.data))
+        return out
+
+    def ttmc_rows(self, Ut, R, mode):
+        keep, ptrs = self._Ut(Ut)
+        r = _shape_arr(R)
+        Y = np.zeros((self.shape[mode], self._kron_len(R, mode)))
+        _lib.check(self.lib.dt_sp_ttmc_rows(self.ctx.h, self.h, ptrs, _i64p(r), mode,
+                                            Y.ctypes.data))
+        return Y
+
+    def hooi(self, R, max_sweeps, Ut0):
+        Ut = [np.ascontiguousarray(u, dtype=np.float64).copy() for u in Ut0]
+        ptrs = (ctypes.c_void_p * self.ndim)(*[a.ctypes.data for a in Ut])
+        r = _shape_arr(R)
+        last = self.ndim - 1
+        G = np.zeros((self._kron_len(R, last), int(R[last])), order="F")
+        rep = HooiReport()
+        _lib.check(self.lib.dt_sp_hooi(self.ctx.h, self.h, _i64p(r), max_sweeps, ptrs,
+                                       G.ctypes.data, ctypes.byref(rep)))
+        return G, Ut, rep.as_dict()

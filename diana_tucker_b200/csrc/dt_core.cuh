@@ -1,0 +1,152 @@
+// Shared host-side machinery of libdt_cuda.so: the context, error handling,
+// host/device pointer staging and launch accounting.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "dt_cuda.h"
+
+struct dt_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    int num_sms = 0;
+    int64_t launches = 0;
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+};
+
+namespace dt {
+
+// Internal failures are C++ exceptions; every extern "C" entry point converts
+// them into a status code plus the thread-local message of dt_last_error().
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+std::string fmt(const char *f, ...);
+void set_last_error(const std::string &msg);
+void clear_last_error();
+
+[[noreturn]] inline void fail(int code, const std::string &msg) { throw Error(code, msg); }
+
+#define DT_CHECK_ARG(cond, ...)                                            \
+    do {                                                                   \
+        if (!(cond)) ::dt::fail(DT_ERR_ARG, ::dt::fmt(__VA_ARGS__));       \
+    } while (0)
+
+#define DT_CUDA(expr)                                                      \
+    do {                                                                   \
+        cudaError_t e_ = (expr);                                           \
+        if (e_ != cudaSuccess)                                             \
+            ::dt::fail(e_ == cudaErrorMemoryAllocation ? DT_ERR_NOMEM      \
+                                                       : DT_ERR_CUDA,      \
+                       ::dt::fmt("%s failed: %s (%s:%d)", #expr,           \
+                                 cudaGetErrorString(e_), __FILE__,         \
+                                 __LINE__));                               \
+    } while (0)
+
+// Every kernel launch goes through this so the context can report how many
+// of this library's kernels a call ran, and launch errors surface at once.
+#define DT_LAUNCH(ctx, kernel, grid, block, smem, ...)                     \
+    do {                                                                   \
+        kernel<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__);   \
+        (ctx)->launches++;                                                 \
+        DT_CUDA(cudaGetLastError());                                       \
+    } while (0)
+
+// Runs fn() and converts a thrown dt::Error into a status code.
+template <class F>
+int guard(F &&fn) {
+    try {
+        clear_last_error();
+        fn();
+        return DT_OK;
+    } catch (const Error &e) {
+        set_last_error(e.what());
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        set_last_error("host allocation failed");
+        return DT_ERR_NOMEM;
+    } catch (const std::exception &e) {
+        set_last_error(e.what());
+        return DT_ERR_CUDA;
+    }
+}
+
+inline void check_ctx(const dt_ctx *ctx) {
+    if (!ctx) fail(DT_ERR_ARG, "null dt_ctx");
+}
+
+bool is_device_ptr(const void *p);
+
+// Stream-ordered device allocation owned by one call.
+class DevMem {
+   public:
+    DevMem() = default;
+    DevMem(dt_ctx *ctx, size_t bytes) { alloc(ctx, bytes); }
+    DevMem(const DevMem &) = delete;
+    DevMem &operator=(const DevMem &) = delete;
+    DevMem(DevMem &&o) noexcept { swap(o); }
+    DevMem &operator=(DevMem &&o) noexcept {
+        release();
+        swap(o);
+        return *this;
+    }
+    ~DevMem() { release(); }
+    void alloc(dt_ctx *ctx, size_t bytes);
+    void release();
+    template <class T>
+    T *as() const { return static_cast<T *>(p_); }
+    void *get() const { return p_; }
+    size_t bytes() const { return bytes_; }
+
+   private:
+    void swap(DevMem &o) {
+        std::swap(p_, o.p_);
+        std::swap(bytes_, o.bytes_);
+        std::swap(ctx_, o.ctx_);
+    }
+    void *p_ = nullptr;
+    size_t bytes_ = 0;
+    dt_ctx *ctx_ = nullptr;
+};
+
+// A caller buffer seen from the device: device pointers pass through, host
+// pointers are staged (copied in for inputs, copied back by finish() for
+// outputs).
+class DevView {
+   public:
+    DevView(dt_ctx *ctx, const void *p, size_t bytes, bool is_input, bool is_output);
+    void *ptr() const { return dptr_; }
+    template <class T>
+    T *as() const { return static_cast<T *>(dptr_); }
+    // For host outputs: copy back and synchronise.
+    void finish();
+
+   private:
+    dt_ctx *ctx_;
+    void *user_;
+    void *dptr_;
+    size_t bytes_;
+    bool output_;
+    bool staged_;
+    DevMem mem_;
+};
+
+inline int64_t prod(const int64_t *s, int n) {
+    int64_t p = 1;
+    for (int i = 0; i < n; i++) p *= s[i];
+    return p;
+}
+
+inline unsigned ceil_div(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
+
+}  // namespace dt

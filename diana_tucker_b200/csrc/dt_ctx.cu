@@ -1,0 +1,130 @@
+// Context lifetime, error reporting and host/device staging.
+#include "dt_core.cuh"
+
+namespace dt {
+
+static thread_local std::string g_last_error;
+
+std::string fmt(const char *f, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, f);
+    vsnprintf(buf, sizeof(buf), f, ap);
+    va_end(ap);
+    return std::string(buf);
+}
+
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+void clear_last_error() { g_last_error.clear(); }
+
+bool is_device_ptr(const void *p) {
+    if (!p) return false;
+    cudaPointerAttributes attr;
+    cudaError_t e = cudaPointerGetAttributes(&attr, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+void DevMem::alloc(dt_ctx *ctx, size_t bytes) {
+    release();
+    ctx_ = ctx;
+    bytes_ = bytes;
+    if (bytes == 0) return;
+    DT_CUDA(cudaMallocAsync(&p_, bytes, ctx->stream));
+}
+
+void DevMem::release() {
+    if (p_ && ctx_) cudaFreeAsync(p_, ctx_->stream);
+    p_ = nullptr;
+    bytes_ = 0;
+}
+
+DevView::DevView(dt_ctx *ctx, const void *p, size_t bytes, bool is_input, bool is_output)
+    : ctx_(ctx), user_(const_cast<void *>(p)), dptr_(nullptr), bytes_(bytes),
+      output_(is_output), staged_(false) {
+    if (bytes == 0) return;
+    if (!p) fail(DT_ERR_ARG, "null buffer");
+    if (is_device_ptr(p)) {
+        dptr_ = user_;
+        return;
+    }
+    staged_ = true;
+    mem_.alloc(ctx, bytes);
+    dptr_ = mem_.get();
+    if (is_input)
+        DT_CUDA(cudaMemcpyAsync(dptr_, p, bytes, cudaMemcpyHostToDevice, ctx->stream));
+}
+
+void DevView::finish() {
+    if (output_ && staged_ && bytes_) {
+        DT_CUDA(cudaMemcpyAsync(user_, dptr_, bytes_, cudaMemcpyDeviceToHost, ctx_->stream));
+        DT_CUDA(cudaStreamSynchronize(ctx_->stream));
+    }
+}
+
+}  // namespace dt
+
+using namespace dt;
+
+extern "C" {
+
+const char *dt_last_error(void) { return g_last_error.c_str(); }
+
+int dt_ctx_create(int device, dt_ctx **out) {
+    return guard([&] {
+        DT_CHECK_ARG(out, "dt_ctx_create: null output pointer");
+        int n = 0;
+        DT_CUDA(cudaGetDeviceCount(&n));
+        DT_CHECK_ARG(device >= 0 && device < n, "dt_ctx_create: device %d out of range (%d)",
+                     device, n);
+        DT_CUDA(cudaSetDevice(device));
+        cudaDeviceProp prop;
+        DT_CUDA(cudaGetDeviceProperties(&prop, device));
+        if (prop.major < 10)
+            fail(DT_ERR_UNSUPPORTED,
+                 fmt("device %d is sm_%d%d; this library is built for sm_100a", device,
+                     prop.major, prop.minor));
+        auto *ctx = new dt_ctx();
+        ctx->device = device;
+        ctx->num_sms = prop.multiProcessorCount;
+        DT_CUDA(cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking));
+        ctx->stream = ctx->own_stream;
+        DT_CUDA(cudaEventCreate(&ctx->ev_start));
+        DT_CUDA(cudaEventCreate(&ctx->ev_stop));
+        *out = ctx;
+    });
+}
+
+int dt_ctx_destroy(dt_ctx *ctx) {
+    return guard([&] {
+        if (!ctx) return;
+        cudaSetDevice(ctx->device);
+        if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+        if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
+        if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
+        if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+        delete ctx;
+    });
+}
+
+int dt_ctx_set_stream(dt_ctx *ctx, void *stream) {
+    return guard([&] {
+        check_ctx(ctx);
+        ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    });
+}
+
+int dt_ctx_synchronize(dt_ctx *ctx) {
+    return guard([&] {
+        check_ctx(ctx);
+        DT_CUDA(cudaSetDevice(ctx->device));
+        DT_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+int64_t dt_ctx_kernel_launches(dt_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+}  // extern "C"

@@ -1,0 +1,347 @@
+// Dense HOOI driver: Algorithm::Tucker::HOOI_ALS
+// (template/algorithm/tucker/hooi_als.tpp:64-123) on one GPU.
+//
+// Per sweep the reference copies A and runs the full TTM chain for every mode
+// (hooi_als.tpp:96-101), then recomputes the core from A (:105-109).  Here the
+// chains share work through a dimension tree: the node owning modes [lo, hi)
+// holds T = X x_{m not in [lo,hi)} U_m^T; its children contract the other half,
+// so X itself is read twice per sweep whatever N is.  The core of a sweep is
+// G = Y_{N-1} x_{N-1} U_{N-1}^T, the last leaf's chain output contracted once
+// more -- the same tensor as the reference's recomputation.  The leading
+// subspace of Y_(n) Y_(n)^T (ALS_, hooi_als.tpp:7-34: five subspace-iteration
+// steps from the previous U_n) runs on the device from the Gram.
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <numeric>
+
+#include "dt_hooi.cuh"
+#include "dt_kernels.cuh"
+
+namespace dt {
+
+namespace {
+
+// Marsaglia polar draw on libc rand() -- the generator the reference's
+// Util::randn (src/util.cpp:10-18) uses for HOOI's initial factors, kept
+// identical so DT_INIT_RANDN_LIBC starts from the reference's factors.
+double libc_polar_randn() {
+    for (;;) {
+        const double u = ((double)rand() / (RAND_MAX)) * 2 - 1;
+        const double v = ((double)rand() / (RAND_MAX)) * 2 - 1;
+        const double r = u * u + v * v;
+        if (r == 0 || r > 1) continue;
+        return u * std::sqrt(-2 * std::log(r) / r);
+    }
+}
+
+// Deterministic N(0,1) for HOSVD's subspace-iteration start (splitmix64 +
+// Box-Muller).
+std::vector<double> seeded_gaussian(size_t n, uint64_t seed) {
+    std::vector<double> out(n);
+    uint64_t s = seed * 0x9E3779B97F4A7C15ULL + 0x1234567ULL;
+    auto next = [&]() {
+        uint64_t z = (s += 0x9E3779B97F4A7C15ULL);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+        return z ^ (z >> 31);
+    };
+    for (size_t i = 0; i < n; i += 2) {
+        const double u1 = ((next() >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+        const double u2 = ((next() >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+        const double rad = std::sqrt(-2.0 * std::log(u1));
+        out[i] = rad * std::cos(6.283185307179586 * u2);
+        if (i + 1 < n) out[i + 1] = rad * std::sin(6.283185307179586 * u2);
+    }
+    return out;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// FP64 engine
+// ---------------------------------------------------------------------------
+void DenseHooi::setup(dt_ctx *c, const void *X, int dt, int n, const int64_t *shp,
+                      const int64_t *rk, const dt_hooi_opts &o) {
+    ctx = c;
+    dtype = dt;
+    N = n;
+    opts = o;
+    for (int m = 0; m < N; m++) {
+        I[m] = shp[m];
+        R[m] = rk[m];
+    }
+    xsize = prod(I, N);
+    Xdev = X;
+    U.resize(N);
+    for (int m = 0; m < N; m++) U[m].alloc(ctx, I[m] * R[m] * sizeof(double));
+    int64_t maxI = 0, maxR = 0;
+    for (int m = 0; m < N; m++) {
+        maxI = std::max(maxI, I[m]);
+        maxR = std::max(maxR, R[m]);
+    }
+    S.alloc(ctx, maxI * maxI * sizeof(double));
+    work.alloc(ctx, (3 * maxI * maxR + maxR + 64) * sizeof(double));
+    flag.alloc(ctx, sizeof(int));
+    scal.alloc(ctx, 4 * sizeof(double));
+    DT_CUDA(cudaMemsetAsync(flag.get(), 0, sizeof(int), ctx->stream));
+    if (dtype == DT_F32 && N == 1) {
+        X64.alloc(ctx, xsize * sizeof(double));
+        f32_to_f64(ctx, static_cast<const float *>(X), xsize, X64.as<double>());
+        Xdev = X64.get();
+        dtype = DT_F64;
+    }
+}
+
+// Contract `t` (shape `shape`) over mode m with U_m^T into a new buffer.
+DevMem DenseHooi::contract(const void *t, int tdtype, int64_t *shape, int m) {
+    int64_t L = 1, B = 1;
+    for (int k = 0; k < m; k++) L *= shape[k];
+    for (int k = m + 1; k < N; k++) B *= shape[k];
+    DevMem out(ctx, L * R[m] * B * sizeof(double));
+    if (tdtype == DT_F32)
+        ttm_f64<float>(ctx, static_cast<const float *>(t), L, shape[m], B, U[m].as<double>(),
+                       I[m], 1, R[m], out.as<double>());
+    else
+        ttm_f64<double>(ctx, static_cast<const double *>(t), L, shape[m], B,
+                        U[m].as<double>(), I[m], 1, R[m], out.as<double>());
+    shape[m] = R[m];
+    return out;
+}
+
+// Contract the modes in `modes` (largest size reduction first).
+DevMem DenseHooi::contract_all(const void *t, int tdtype, int64_t *shape,
+                               std::vector<int> modes) {
+    std::sort(modes.begin(), modes.end(), [&](int a, int b) {
+        return (double)I[a] / R[a] > (double)I[b] / R[b];
+    });
+    DevMem cur;
+    const void *src = t;
+    int sdt = tdtype;
+    for (int m : modes) {
+        DevMem nxt = contract(src, sdt, shape, m);
+        cur = std::move(nxt);
+        src = cur.get();
+        sdt = DT_F64;
+    }
+    return cur;
+}
+
+void DenseHooi::leaf(int n, const double *Y, const int64_t *shape) {
+    int64_t L = 1, B = 1;
+    for (int k = 0; k < n; k++) L *= shape[k];
+    for (int k = n + 1; k < N; k++) B *= shape[k];
+    ttt_f64(ctx, Y, Y, L, I[n], I[n], B, S.as<double>());
+    subspace_iter(ctx, S.as<double>(), I[n], U[n].as<double>(), R[n], opts.inner_iters,
+                  work.as<double>(), flag.as<int>());
+    if (n == N - 1) {
+        // Core of this sweep: G = Y x_{N-1} U_{N-1}^T (hooi_als.tpp:105-109).
+        G.alloc(ctx, L * R[n] * sizeof(double));
+        ttm_f64<double>(ctx, Y, L, I[n], 1, U[n].as<double>(), I[n], 1, R[n], G.as<double>());
+        sumsq(ctx, G.get(), DT_F64, L * R[n], scal.as<double>() + 1);
+    }
+}
+
+void DenseHooi::node(int lo, int hi, const void *T, int tdtype, const int64_t *shape) {
+    if (hi - lo == 1) {
+        leaf(lo, static_cast<const double *>(T), shape);
+        return;
+    }
+    const int mid = (lo + hi) / 2;
+    for (int side = 0; side < 2; side++) {
+        const int clo = side == 0 ? lo : mid, chi = side == 0 ? mid : hi;
+        std::vector<int> modes;
+        for (int m = lo; m < hi; m++)
+            if (m < clo || m >= chi) modes.push_back(m);
+        int64_t cshape[16];
+        std::memcpy(cshape, shape, N * sizeof(int64_t));
+        DevMem child = contract_all(T, tdtype, cshape, modes);
+        node(clo, chi, child.get(), DT_F64, cshape);
+    }
+}
+
+void DenseHooi::sweep() {
+    if (N == 1) {
+        leaf(0, static_cast<const double *>(Xdev), I);
+        return;
+    }
+    int64_t shape[16];
+    std::memcpy(shape, I, N * sizeof(int64_t));
+    node(0, N, Xdev, dtype, shape);
+}
+
+void DenseHooi::init_factors(double *const *U_user) {
+    if (opts.init == DT_INIT_GIVEN) {
+        DT_CHECK_ARG(U_user, "DT_INIT_GIVEN needs initial factors in U");
+        for (int m = 0; m < N; m++) {
+            DT_CHECK_ARG(U_user[m], "DT_INIT_GIVEN: U[%d] is NULL", m);
+            DevView u(ctx, U_user[m], I[m] * R[m] * sizeof(double), true, false);
+            DT_CUDA(cudaMemcpyAsync(U[m].get(), u.ptr(), I[m] * R[m] * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, ctx->stream));
+        }
+        return;
+    }
+    if (opts.init == DT_INIT_RANDN_LIBC) {
+        // hooi_als.tpp:74-81: U_rand(I_n x R_n).randn(); U_n = Q of reduced_QR.
+        srand(opts.seed);
+        DevMem tmp(ctx, 0);
+        for (int m = 0; m < N; m++) {
+            std::vector<double> h((size_t)(I[m] * R[m]));
+            for (auto &v : h) v = libc_polar_randn();
+            DevMem a(ctx, h.size() * sizeof(double));
+            DT_CUDA(cudaMemcpyAsync(a.get(), h.data(), h.size() * sizeof(double),
+                                    cudaMemcpyHostToDevice, ctx->stream));
+            DevMem w(ctx, (I[m] * R[m] + R[m]) * sizeof(double));
+            householder_qr(ctx, a.as<double>(), I[m], R[m], U[m].as<double>(), nullptr,
+                           w.as<double>());
+            DT_CUDA(cudaStreamSynchronize(ctx->stream));  // h goes out of scope
+        }
+        return;
+    }
+    // HOSVD: leading R_n eigenvectors of X_(n) X_(n)^T by subspace iteration
+    // from a seeded Gaussian start.
+    const double *X64p = static_cast<const double *>(Xdev);
+    DevMem xconv;
+    if (dtype == DT_F32) {
+        xconv.alloc(ctx, xsize * sizeof(double));
+        f32_to_f64(ctx, static_cast<const float *>(Xdev), xsize, xconv.as<double>());
+        X64p = xconv.as<double>();
+    }
+    for (int m = 0; m < N; m++) {
+        int64_t L = 1, B = 1;
+        for (int k = 0; k < m; k++) L *= I[k];
+        for (int k = m + 1; k < N; k++) B *= I[k];
+        ttt_f64(ctx, X64p, X64p, L, I[m], I[m], B, S.as<double>());
+        std::vector<double> h = seeded_gaussian((size_t)(I[m] * R[m]), 1000 + m);
+        DT_CUDA(cudaMemcpyAsync(U[m].get(), h.data(), h.size() * sizeof(double),
+                                cudaMemcpyHostToDevice, ctx->stream));
+        subspace_iter(ctx, S.as<double>(), I[m], U[m].as<double>(), R[m], hosvd_iters,
+                      work.as<double>(), flag.as<int>());
+        DT_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+}
+
+double DenseHooi::read_scalar(int k) {
+    double h = 0.0;
+    DT_CUDA(cudaMemcpyAsync(&h, scal.as<double>() + k, sizeof(double), cudaMemcpyDeviceToHost,
+                            ctx->stream));
+    DT_CUDA(cudaStreamSynchronize(ctx->stream));
+    return h;
+}
+
+void DenseHooi::run(double *G_user, double *const *U_user, dt_hooi_report *rep) {
+    const int64_t launches0 = ctx->launches;
+    DT_CUDA(cudaEventRecord(ctx->ev_start, ctx->stream));
+    sumsq(ctx, Xdev, dtype, xsize, scal.as<double>());
+    init_factors(U_user);
+    const double x2 = read_scalar(0);
+    double prev = -1.0, res = 0.0;
+    int sweeps = 0;
+    for (int it = 0; it < opts.max_sweeps; it++) {
+        sweep();
+        const double g2 = read_scalar(1);
+        res = std::sqrt(std::max(0.0, 1.0 - g2 / x2));
+        if (rep && it < DT_MAX_HIST) rep->res_hist[it] = res;
+        sweeps = it + 1;
+        if (opts.verbose)
+            fprintf(stderr, "[dt_hooi] sweep %d  ||G|| = %.12e  residual = %.12e\n", it + 1,
+                    std::sqrt(g2), res);
+        if (opts.tol > 0 && prev >= 0 && std::fabs(res - prev) < opts.tol) break;
+        prev = res;
+    }
+    if (sweeps == 0) {
+        // No sweep requested: the core of the initial factors.
+        int64_t shape[16];
+        std::memcpy(shape, I, N * sizeof(int64_t));
+        std::vector<int> all(N);
+        std::iota(all.begin(), all.end(), 0);
+        G = contract_all(Xdev, dtype, shape, all);
+        sumsq(ctx, G.get(), DT_F64, prod(R, N), scal.as<double>() + 1);
+    }
+    DT_CUDA(cudaEventRecord(ctx->ev_stop, ctx->stream));
+    const double g2 = read_scalar(1);
+    int fl = 0;
+    DT_CUDA(cudaMemcpyAsync(&fl, flag.get(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    DT_CUDA(cudaStreamSynchronize(ctx->stream));
+    float ms = 0.f;
+    DT_CUDA(cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop));
+    if (!std::isfinite(g2)) fail(DT_ERR_NUMERIC, "HOOI produced a non-finite core");
+    if (G_user) {
+        DevView g(ctx, G_user, prod(R, N) * sizeof(double), false, true);
+        DT_CUDA(cudaMemcpyAsync(g.ptr(), G.get(), prod(R, N) * sizeof(double),
+                                cudaMemcpyDeviceToDevice, ctx->stream));
+        g.finish();
+    }
+    if (U_user) {
+        for (int m = 0; m < N; m++) {
+            if (!U_user[m]) continue;
+            DevView u(ctx, U_user[m], I[m] * R[m] * sizeof(double), false, true);
+            DT_CUDA(cudaMemcpyAsync(u.ptr(), U[m].get(), I[m] * R[m] * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, ctx->stream));
+            u.finish();
+        }
+    }
+    DT_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (rep) {
+        rep->sweeps = sweeps;
+        rep->x_norm = std::sqrt(x2);
+        rep->g_norm = std::sqrt(g2);
+        rep->residual = std::sqrt(std::max(0.0, 1.0 - g2 / x2));
+        rep->device_ms = ms;
+        rep->kernel_launches = (int)(ctx->launches - launches0);
+    }
+}
+
+}  // namespace dt
+
+using namespace dt;
+
+extern "C" {
+
+void dt_hooi_default_opts(dt_hooi_opts *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->init = DT_INIT_RANDN_LIBC;
+    o->seed = 1;
+    o->max_sweeps = 5;
+    o->tol = 0.0;
+    o->inner_iters = 5;
+    o->precision = DT_PREC_FP64;
+    o->refine_sweeps = 0;
+    o->verbose = 0;
+}
+
+int dt_hooi_dense(dt_ctx *ctx, const void *X, int dtype, int ndim, const int64_t *shape,
+                  const int64_t *ranks, const dt_hooi_opts *opts, double *G,
+                  double *const *U, dt_hooi_report *report) {
+    return guard([&] {
+        check_ctx(ctx);
+        DT_CHECK_ARG(X && shape && ranks, "dt_hooi_dense: null argument");
+        DT_CHECK_ARG(ndim >= 1 && ndim <= 16, "dt_hooi_dense: ndim %d out of range", ndim);
+        DT_CHECK_ARG(dtype == DT_F64 || dtype == DT_F32, "dt_hooi_dense: bad dtype %d", dtype);
+        for (int m = 0; m < ndim; m++)
+            DT_CHECK_ARG(shape[m] >= 1 && ranks[m] >= 1 && ranks[m] <= shape[m],
+                         "dt_hooi_dense: need 1 <= R_%d <= I_%d (R=%lld, I=%lld)", m, m,
+                         (long long)ranks[m], (long long)shape[m]);
+        dt_hooi_opts o;
+        if (opts)
+            o = *opts;
+        else
+            dt_hooi_default_opts(&o);
+        DT_CHECK_ARG(o.max_sweeps >= 0, "dt_hooi_dense: max_sweeps must be >= 0");
+        DT_CHECK_ARG(o.inner_iters >= 1, "dt_hooi_dense: inner_iters must be >= 1");
+        DT_CUDA(cudaSetDevice(ctx->device));
+        if (report) std::memset(report, 0, sizeof(*report));
+        const size_t esz = dtype == DT_F64 ? 8 : 4;
+        DevView x(ctx, X, prod(shape, ndim) * esz, true, false);
+        if (o.precision == DT_PREC_FP64) {
+            DenseHooi h;
+            h.setup(ctx, x.ptr(), dtype, ndim, shape, ranks, o);
+            h.run(G, U, report);
+        } else {
+            hooi_dense_lowprec(ctx, x.ptr(), dtype, ndim, shape, ranks, o, G, U, report);
+        }
+    });
+}
+
+}  // extern "C"

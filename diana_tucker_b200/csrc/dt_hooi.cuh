@@ -1,0 +1,45 @@
+// Dense HOOI drivers (FP64 and the tensor-core mixed-precision variant).
+#pragma once
+
+#include <algorithm>
+#include <vector>
+
+#include "dt_core.cuh"
+
+namespace dt {
+
+// The FP64 HOOI: CUDA-core TTM chain over a dimension tree, FP64 Gram and
+// subspace iteration.  X may be FP64 or FP32 (read as FP32, computed in FP64).
+struct DenseHooi {
+    dt_ctx *ctx = nullptr;
+    int dtype = DT_F64;
+    int N = 0;
+    int64_t I[16] = {}, R[16] = {};
+    int64_t xsize = 0;
+    dt_hooi_opts opts{};
+    const void *Xdev = nullptr;
+    DevMem X64;               // FP64 copy when needed
+    std::vector<DevMem> U;    // I_n x R_n col-major
+    DevMem S, work, flag, scal, G;
+    int hosvd_iters = 30;
+
+    void setup(dt_ctx *c, const void *X, int dtype, int n, const int64_t *shape,
+               const int64_t *ranks, const dt_hooi_opts &o);
+    void init_factors(double *const *U_user);
+    void run(double *G_user, double *const *U_user, dt_hooi_report *rep);
+
+   private:
+    DevMem contract(const void *t, int tdtype, int64_t *shape, int m);
+    DevMem contract_all(const void *t, int tdtype, int64_t *shape, std::vector<int> modes);
+    void node(int lo, int hi, const void *T, int tdtype, const int64_t *shape);
+    void leaf(int n, const double *Y, const int64_t *shape);
+    void sweep();
+    double read_scalar(int k);
+};
+
+// BF16 / split-BF16 tensor-core HOOI (dt_hooi_tc.cu).
+void hooi_dense_lowprec(dt_ctx *ctx, const void *X, int dtype, int ndim, const int64_t *shape,
+                        const int64_t *ranks, const dt_hooi_opts &opts, double *G,
+                        double *const *U, dt_hooi_report *report);
+
+}  // namespace dt

@@ -1,0 +1,207 @@
+/*
+ * dt_cuda.h -- C ABI of libdt_cuda.so, the B200 (sm_100a) implementation of
+ * DIANA-Tucker's HOOI-ALS hot path.
+ *
+ * Conventions (mirroring the reference's Operator<double> seam,
+ * include/operator.hpp:8-70, and its Tensor<Ty> layout, template/tensor_mpi.tpp:49-53):
+ *  - dense tensors are column-major (mode 0 fastest), shapes are int64;
+ *  - a matrix argument "J x I col-major" is stored with its row index fastest;
+ *  - every pointer may be HOST or DEVICE memory of the context's GPU; host
+ *    buffers are staged through the context (the reference's buffers are
+ *    malloc'd host memory, operator_cpu.tpp:6-12);
+ *  - every entry point returns 0 on success and a nonzero DT_ERR_* code on
+ *    failure; dt_last_error() then describes the failure.  This replaces the
+ *    reference's error()/assert -> exit() convention (include/logger.hpp:75-123);
+ *  - a context is bound to one device and one CUDA stream; use one context
+ *    per host thread.
+ *  - the world has size 1: the reference's MPI distribution
+ *    (DistributionCartesianBlock, communicator.tpp) collapses to one GPU.
+ */
+#ifndef DT_CUDA_H
+#define DT_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define DT_API __attribute__((visibility("default")))
+#else
+#define DT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define DT_OK 0
+#define DT_ERR_ARG 1       /* invalid argument (shape mismatch, bad mode, ...) */
+#define DT_ERR_CUDA 2      /* a CUDA runtime / driver call failed */
+#define DT_ERR_NOMEM 3     /* device allocation failed */
+#define DT_ERR_NUMERIC 4   /* breakdown (singular matrix, non-SPD Gram, NaN) */
+#define DT_ERR_UNSUPPORTED 5
+
+/* ---- element types and options --------------------------------------- */
+#define DT_F64 0
+#define DT_F32 1
+
+/* HOOI initialisation */
+#define DT_INIT_RANDN_LIBC 0 /* reference: srand(seed); Util::randn() per element,
+                                column-major I_n x R_n, then reduced_QR
+                                (hooi_als.tpp:74-81, util.cpp:10-18) */
+#define DT_INIT_HOSVD 1      /* leading R_n eigenvectors of X_(n) X_(n)^T */
+#define DT_INIT_GIVEN 2      /* factors supplied by the caller in U */
+
+/* HOOI arithmetic for the TTM chain and the Gram (the eigensolve / QR, the
+ * fit and the final core projection are FP64 in every mode). */
+#define DT_PREC_FP64 0   /* FP64 CUDA-core kernels throughout (the drop-in) */
+#define DT_PREC_BF16 1   /* tcgen05 BF16 x BF16 -> FP32 TTM chain and Gram */
+#define DT_PREC_BF16X2 2 /* tcgen05 with split hi+lo BF16 operands (~2^-16) */
+
+typedef struct dt_ctx dt_ctx;
+
+typedef struct {
+    int init;           /* DT_INIT_* */
+    unsigned seed;      /* for DT_INIT_RANDN_LIBC */
+    int max_sweeps;     /* reference: max_iter */
+    double tol;         /* stop when |res_k - res_{k-1}| < tol; <= 0 runs max_sweeps */
+    int inner_iters;    /* subspace iterations per mode (reference ALS_: 5) */
+    int precision;      /* DT_PREC_* */
+    int refine_sweeps;  /* BF16 modes: the last sweeps (after the tol test first
+                           passes) run with hi+lo operands; 0 = none */
+    int verbose;        /* print one line per sweep to stderr */
+} dt_hooi_opts;
+
+#define DT_MAX_HIST 256
+typedef struct {
+    int sweeps;                   /* sweeps run */
+    double x_norm;                /* ||X||_F (FP64) */
+    double g_norm;                /* ||G||_F of the returned core (FP64 projection) */
+    double residual;              /* sqrt(1 - ||G||^2/||X||^2) */
+    double device_ms;             /* CUDA-event time of the whole decomposition */
+    double res_hist[DT_MAX_HIST]; /* per-sweep residual as tracked by the sweep */
+    int kernel_launches;          /* kernels launched by the decomposition */
+} dt_hooi_report;
+
+/* ---- context ---------------------------------------------------------- */
+/* No reference counterpart (the reference has no device state). */
+DT_API int dt_ctx_create(int device, dt_ctx **ctx);
+DT_API int dt_ctx_destroy(dt_ctx *ctx);
+/* Run all work of this context on the given cudaStream_t (NULL = the
+ * context's own stream). */
+DT_API int dt_ctx_set_stream(dt_ctx *ctx, void *stream);
+DT_API int dt_ctx_synchronize(dt_ctx *ctx);
+/* Message of the last failure on the calling thread ("" if none). */
+DT_API const char *dt_last_error(void);
+/* Number of this library's kernels launched by ctx since creation. */
+DT_API int64_t dt_ctx_kernel_launches(dt_ctx *ctx);
+
+/* ---- operator-level entry points -------------------------------------- */
+/* Y = X x_mode M, M is J x I_mode col-major, Y has shape[mode] replaced by J.
+ * Replaces Function::ttm (template/function/tensor.tpp:272-335) at world size 1,
+ * without its tenmatt/mattten permute copies (operator_cpu.tpp:83-135). */
+DT_API int dt_ttm_f64(dt_ctx *ctx, const double *X, int ndim, const int64_t *shape, int mode,
+               const double *M, int64_t J, double *Y);
+
+/* G = X_(mode) X_(mode)^T, I_mode x I_mode col-major.
+ * Replaces Function::gram (tensor.tpp:18-120). */
+DT_API int dt_gram_f64(dt_ctx *ctx, const double *X, int ndim, const int64_t *shape, int mode,
+                double *G);
+
+/* C = A_(mode) B_(mode)^T, shapeA[mode] x shapeB[mode] col-major; the other
+ * modes of A and B must agree.  Replaces Function::ttt_except (tensor.tpp:132-259). */
+DT_API int dt_ttt_except_f64(dt_ctx *ctx, const double *A, const int64_t *shapeA, const double *B,
+                      const int64_t *shapeB, int ndim, int mode, double *C);
+
+/* ||X||_F.  Replaces Function::fnorm (tensor.tpp:467-480) / Operator::fnorm
+ * (operator_double.cpp:74-82). */
+DT_API int dt_fnorm_f64(dt_ctx *ctx, const double *X, int64_t n, double *out);
+
+/* C = op(A) op(B), column-major; trans = 0 (N) or 1 (T).  (m,n,k) as in the
+ * reference: NN C(m x n) = A(m x k) B(k x n); NT C = A(m x k) B(n x k)^T;
+ * TN C = A(k x m)^T B(k x n).  Replaces Operator::matmulNN/NT/TN
+ * (operator_double.cpp:157-216). */
+DT_API int dt_matmul_f64(dt_ctx *ctx, int transA, int transB, int64_t m, int64_t n, int64_t k,
+                  const double *A, const double *B, double *C);
+
+/* Householder QR of an m x n (m >= n) col-major matrix: Q m x n, R n x n
+ * (R may be NULL).  Same reflector convention as LAPACK dgeqrf/dorgqr.
+ * Replaces Operator::QR (operator_double.cpp:131-155). */
+DT_API int dt_reduced_qr_f64(dt_ctx *ctx, const double *A, int64_t m, int64_t n, double *Q,
+                      double *R);
+
+/* Inverse of an n x n matrix by LU with partial pivoting.
+ * Replaces Operator::inverse (operator_double.cpp:84-103); a zero pivot
+ * returns DT_ERR_NUMERIC where the reference only warns. */
+DT_API int dt_inverse_f64(dt_ctx *ctx, const double *A, int64_t n, double *Ainv);
+
+/* Modified Gram-Schmidt over the len1 rows of a len1 x len2 col-major matrix,
+ * in place.  Replaces Operator::orth2 (operator_double.cpp:248-277). */
+DT_API int dt_orth2_f64(dt_ctx *ctx, double *A, int64_t len1, int64_t len2);
+
+/* ALS_ leading-subspace step for mode n of the TTM-chain output Y, from the
+ * I_n x R col-major L0: Q = orth((Y_(n) Y_(n)^T)^iters L0).  Replaces
+ * Algorithm::Tucker::ALS_ (hooi_als.tpp:7-34), whose 5 steps span the same
+ * subspace. */
+DT_API int dt_als_f64(dt_ctx *ctx, const double *Y, int ndim, const int64_t *shape, int mode,
+               const double *L0, int64_t R, int iters, double *Q);
+
+/* ---- dense HOOI ------------------------------------------------------- */
+/* Tucker decomposition of X (dtype DT_F64 or DT_F32, column-major) with the
+ * given ranks.  G (prod ranks, col-major) and U[n] (shape[n] x ranks[n]
+ * col-major) receive the result; with DT_INIT_GIVEN, U holds the initial
+ * factors on entry.  Either may be NULL.  Replaces
+ * Algorithm::Tucker::HOOI_ALS (hooi_als.tpp:64-123). */
+DT_API int dt_hooi_dense(dt_ctx *ctx, const void *X, int dtype, int ndim, const int64_t *shape,
+                  const int64_t *ranks, const dt_hooi_opts *opts, double *G,
+                  double *const *U, dt_hooi_report *report);
+
+/* Fills opts with the reference's behaviour: random libc init, 5 inner
+ * iterations, FP64, no tolerance. */
+DT_API void dt_hooi_default_opts(dt_hooi_opts *opts);
+
+/* ---- sparse tensors --------------------------------------------------- */
+typedef struct dt_sptensor dt_sptensor;
+
+/* Uploads a COO tensor (idx[m][e], 0-based int64; vals[e] FP64) and builds,
+ * on the device, one copy of the nonzeros sorted by each mode with its row
+ * pointer (the per-mode CSR that SpTensor::index_buffer declares,
+ * include/sp_tensor.hpp:16-24, and ttmc_mTL reads as v_index_buffer).
+ * Replaces SpTensor<Ty>::SpTensor(data_buffer<Ty>*) (sp_tensor.hpp:71-240)
+ * at world size 1. */
+DT_API int dt_sptensor_create(dt_ctx *ctx, int64_t nnz, int ndim, const int64_t *const *idx,
+                       const double *vals, const int64_t *shape, dt_sptensor **sp);
+DT_API int dt_sptensor_destroy(dt_sptensor *sp);
+/* ||A||_F of the nonzeros.  Replaces Function::fnorm(SpTensor) (sp_tensor.tpp:6-14). */
+DT_API int dt_sp_fnorm(dt_ctx *ctx, const dt_sptensor *sp, double *out);
+
+/* Factors are TRANSPOSED as in the reference (sp_hooi_als.tpp:80): Ut[m] is
+ * R_m x I_m col-major, i.e. factor row i is contiguous at Ut[m] + i*R_m.
+ * P = prod_{m != mode} R_m, Kronecker index with the lowest mode fastest
+ * (sp_tensor.tpp:367-417). */
+
+/* L (P x R_mode col-major) = Y_(mode)^T U_mode.  Replaces Function::ttmc_mTR
+ * (sp_tensor.tpp:236-286), intended semantics. */
+DT_API int dt_sp_ttmc_mTR(dt_ctx *ctx, const dt_sptensor *sp, const double *const *Ut,
+                   const int64_t *R, int mode, double *L);
+/* out (R_mode x I_mode col-major) = (Y_(mode) L)^T.  Replaces
+ * Function::ttmc_mTL (sp_tensor.tpp:288-365). */
+DT_API int dt_sp_ttmc_mTL(dt_ctx *ctx, const dt_sptensor *sp, const double *const *Ut,
+                   const int64_t *R, int mode, const double *L, double *out);
+/* Y_(mode) rows: Y is I_mode x P row-major (row i contiguous).  The TTMc
+ * itself (add_outer_product_all over each row, sp_tensor.tpp:367-417). */
+DT_API int dt_sp_ttmc_rows(dt_ctx *ctx, const dt_sptensor *sp, const double *const *Ut,
+                    const int64_t *R, int mode, double *Y);
+
+/* Sparse HOOI power sweeps: per mode L = Y_(n)^T U_n, U_n <- orth(Y_(n) L);
+ * core G (P_{N-1} x R_{N-1} col-major = the core tensor col-major) after the
+ * sweeps.  Ut holds the initial transposed factors on entry and the final
+ * ones on exit.  Replaces Algorithm::SpTucker::Sp_HOOI_ALS
+ * (sp_hooi_als.tpp:67-118). */
+DT_API int dt_sp_hooi(dt_ctx *ctx, const dt_sptensor *sp, const int64_t *R, int max_sweeps,
+               double *const *Ut, double *G, dt_hooi_report *report);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DT_CUDA_H */
