@@ -1,0 +1,391 @@
+#!/usr/bin/env python
+"""HOOI time-to-FP64-rel-err on one B200 per rank.
+
+Workload: the 96x96x96x96 FP32 Tucker tensor (core 16^4 N(0,1) scaled by
+0.9^(i+j+k+l), QR'd Gaussian factors, noise N(0,1e-6), seed 1), HOOI ranks
+16^4.  A step is one whole decomposition with X resident in HBM: BF16 hi/lo
+split of X, libc-seeded random orthonormal init, BF16 tensor-core sweeps until
+the residual settles, split-BF16 refinement sweeps, FP64 subspace iteration
+per mode, and the final FP64 core projection -- until the relative
+reconstruction error is within 1e-6 of the FP64 oracle's (checked every run).
+
+One JSON line on rank 0:
+  value        ms per decomposition (max over ranks; lower is better)
+  e2e          the same through the public API from pinned host memory
+               (H2D of X and D2H of G and U inside the timed region)
+  fp64_gpu     the plain FP64 GPU path on the same tensor and stopping rule
+  roofline     the X-streaming tensor-core TTM (the dominant kernel):
+               algorithmic bytes / CUDA-event time vs measured HBM copy BW
+  ttmc         sparse TTMc HBM GB/s on the 2e6 x 2e5 x 5e4 Zipf COO tensor
+  cpu_baseline the reference's own HOOI_ALS (compiled from its sources, FP64,
+               all host threads) on a bounded sample of the same tensor
+
+--impl reference runs the reference's CPU HOOI instead (rank 0 only).
+Multi-GPU: replicas (each rank decomposes its own copy; no collective on the
+data path; barrier + max-over-ranks timing only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "HOOI time-to-FP64-rel-err (BF16-TC+FP64 vs FP64 GPU); TTMc HBM GB/s"
+RANKS = (16, 16, 16, 16)
+SHAPE = (96, 96, 96, 96)
+TARGET = 1e-6
+FALLBACK_HBM_GBS = 6650.0
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def _oracle_residual():
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "large_oracle.json")) as f:
+            d = json.load(f)["dense_96x4_r16"]
+        return float(d["residual"]), int(d["sweeps"])
+    except Exception:
+        return None, None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _dist_setup(n_gpus):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def _max_over_ranks(v, world, device):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{device}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(world, device):
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        dist.barrier(device_ids=[device])
+        torch.cuda.synchronize()
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    from diana_tucker_b200 import DT_PREC_BF16, DT_PREC_FP64, Context, datasets
+
+    world, rank, local = _dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    ctx = Context(local)
+    X = datasets.dense_96x4_fp32()
+    flat = np.ascontiguousarray(X.reshape(-1, order="F"))
+    Xd = torch.from_numpy(flat).to(f"cuda:{local}")
+    kw = dict(init="randn", seed=1, max_sweeps=30, tol=1e-9, inner_iters=5, shape=SHAPE)
+
+    def mixed(profile=False):
+        return ctx.hooi_dense(Xd, RANKS, precision=DT_PREC_BF16, refine_sweeps=2,
+                              profile=profile, **kw)
+
+    def fp64(profile=False):
+        return ctx.hooi_dense(Xd, RANKS, precision=DT_PREC_FP64, profile=profile, **kw)
+
+    # Warm-up (module loading, memory pool).
+    for _ in range(args.warmup):
+        mixed()
+    # Timed region: K whole decompositions, device time by CUDA events on the
+    # stream the library runs on, max over ranks.
+    clocks = ClockSampler(local)
+    _barrier(world, local)
+    torch.cuda.synchronize()
+    clocks.start()
+    l0 = ctx.kernel_launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    reps = []
+    for _ in range(args.steps):
+        _, _, rep = mixed(profile=True)
+        reps.append(rep)
+    ev1.record()
+    torch.cuda.synchronize()
+    launches = ctx.kernel_launches() - l0
+    clk = clocks.stop()
+    _barrier(world, local)
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ms = _max_over_ranks(ms, world, local)
+    rep = reps[-1]
+
+    # FP64 GPU path, same tensor and stopping rule.
+    fp64()
+    t64 = []
+    for _ in range(max(1, min(args.steps, 3))):
+        _, _, r64 = fp64(profile=True)
+        t64.append(r64["device_ms"])
+    fp64_ms = float(np.median(t64))
+
+    # End to end through the public API from pinned host memory.
+    Xh = torch.from_numpy(flat).pin_memory()
+    e2e_t = []
+    for i in range(max(1, min(args.steps, 3)) + 1):
+        t0 = time.perf_counter()
+        G, U, _ = ctx.hooi_dense(Xh, RANKS, precision=DT_PREC_BF16, refine_sweeps=2, **kw)
+        dt = (time.perf_counter() - t0) * 1e3
+        if i > 0:
+            e2e_t.append(dt)
+    e2e_ms = _max_over_ranks(float(np.median(e2e_t)), world, local)
+    h2d = flat.nbytes
+    d2h = int(np.prod(RANKS)) * 8 + sum(s * r * 8 for s, r in zip(SHAPE, RANKS))
+
+    oracle_res, oracle_sweeps = _oracle_residual()
+    ref_res = oracle_res if oracle_res is not None else r64["residual"]
+    err = abs(rep["residual"] - ref_res)
+
+    peak, peak_kind = _peaks()
+    per_launch_ms = rep["ttm_x_ms"] / max(1, rep["ttm_x_launches"])
+    per_launch_bytes = rep["ttm_x_bytes"] / max(1, rep["ttm_x_launches"])
+    achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms > 0 else 0.0
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "roofline_traffic.json")) as f:
+            traffic = json.load(f).get("tc_ttm_kernel_x_bf16_per_launch_bytes")
+    except Exception:
+        pass
+
+    out = {
+        "metric": METRIC,
+        "value": round(ms, 4),
+        "unit": "ms",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms, 4),
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "bf16",
+        "data": "synthetic (seeded Tucker tensor, generated in-process)",
+        "config": {
+            "workload": "dense 96x96x96x96 FP32 Tucker(16^4, core*0.9^(i+j+k+l)) + N(0,1e-6), "
+                        "seed 1; HOOI ranks 16^4; BF16 tcgen05 TTM chain + Gram with split "
+                        "hi/lo refinement, FP64 subspace iteration / fit / final core",
+            "init": "libc-seeded Gaussian + QR (seed 1)",
+            "stop": "BF16 sweeps until the residual settles to 1e-3, then 2 split sweeps",
+            "target": f"|rel-err - FP64 oracle rel-err| <= {TARGET}",
+            "l2": "inputs larger than L2 (X: 340 MB FP32, 170 MB per BF16 half; L2 126 MB)",
+            "parallelism": f"replicas x{world} (no data-path collective)",
+        },
+        "rel_err": rep["residual"],
+        "rel_err_oracle": ref_res,
+        "rel_err_gap": err,
+        "target_met": bool(err <= TARGET),
+        "sweeps": rep["sweeps"],
+        "fp64_gpu": {"ms": round(fp64_ms, 4), "rel_err": r64["residual"], "sweeps": r64["sweeps"],
+                     "speedup_mixed_vs_fp64": round(fp64_ms / ms, 3) if ms > 0 else None},
+        "decompositions_per_s": round(world * 1000.0 / ms, 3) if ms > 0 else None,
+        "e2e": {"value": round(e2e_ms, 4), "unit": "ms", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches // max(1, args.steps)),
+        "gpu_launches_timed_region": int(launches),
+        "roofline": {"kernel": "tc_ttm_kernel (X x_n U^T, BF16 X streamed by TMA)",
+                     "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4) if peak else None,
+                     "traffic": traffic,
+                     "algorithmic_bytes_per_launch": per_launch_bytes,
+                     "launch_ms": per_launch_ms, "launches_per_step": rep["ttm_x_launches"]},
+    }
+    if clk:
+        out["clocks"] = clk
+    if args.ttmc and world == 1:
+        out["ttmc"] = _ttmc(ctx, peak)
+    if rank == 0 and world == 1 and args.cpu:
+        out["cpu_baseline"] = _cpu_baseline(X, oracle_sweeps or r64["sweeps"])
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def _ttmc(ctx, peak):
+    """Sparse TTMc bandwidth on the 2,000,000 x 200,000 x 50,000 COO tensor
+    (50M Zipf(1.1) draws, merged), ranks 16^3: one sparse HOOI sweep with the
+    TTMc launches timed by CUDA events."""
+    from diana_tucker_b200 import datasets
+    t0 = time.time()
+    idx, vals, shape = datasets.sparse_2m_200k_50k()
+    gen_s = time.time() - t0
+    sp = ctx.sptensor(idx, vals, shape)
+    R = (16, 16, 16)
+    Ut = datasets.random_orthonormal_transposed(shape, R, 2)
+    sp.hooi(R, 1, Ut)
+    _, _, rep = sp.hooi(R, 1, Ut, profile=True)
+    gbs = rep["ttm_x_bytes"] / (rep["ttm_x_ms"] * 1e-3) / 1e9 if rep["ttm_x_ms"] else 0.0
+    sp.close()
+    return {"value": round(gbs, 1), "unit": "GB/s", "frac_of_hbm": round(gbs / peak, 4),
+            "nnz": int(len(vals)), "launches": rep["ttm_x_launches"],
+            "ms": rep["ttm_x_ms"], "bytes": rep["ttm_x_bytes"],
+            "sweep_ms": rep["device_ms"], "gen_s": round(gen_s, 1)}
+
+
+def _cpu_baseline(X32, sweeps):
+    """The reference's HOOI_ALS (compiled from its sources with a size-1 MPI
+    shim and OpenBLAS; all host threads) on the same tensor upcast to FP64:
+    one sweep timed, extrapolated to the sweeps the oracle needs."""
+    import numpy as np
+    from oracle import ref
+    if not ref.available():
+        return {"value": None, "unit": "ms", "kind": "reference", "cores": os.cpu_count(),
+                "sample": "unavailable: oracle/_ref/libdiana_ref.so not built"}
+    X = X32.astype(np.float64)
+    t0 = time.perf_counter()
+    ref.hooi_als(X, RANKS, 1, seed=1)
+    one = (time.perf_counter() - t0) * 1e3
+    return {"value": round(one * sweeps, 1), "unit": "ms", "kind": "reference",
+            "cores": os.cpu_count(),
+            "sample": f"one HOOI_ALS sweep (init + 1 sweep + core) = {one:.0f} ms, "
+                      f"x {sweeps} sweeps to converge"}
+
+
+def run_reference(args):
+    """The reference's own CPU HOOI on the same workload (rank 0 only)."""
+    import numpy as np
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from diana_tucker_b200 import datasets
+    from oracle import ref
+    oracle_res, sweeps = _oracle_residual()
+    sweeps = sweeps or 3
+    if not ref.available():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/libdiana_ref.so was not built"}))
+        return
+    X = datasets.dense_96x4_fp32().astype(np.float64)
+    for _ in range(args.warmup):
+        ref.hooi_als(X, RANKS, 1, seed=1)
+    t = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        ref.hooi_als(X, RANKS, 1, seed=1)
+        t.append((time.perf_counter() - t0) * 1e3)
+    one = float(np.median(t))
+    v = one * sweeps
+    out = {
+        "impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": "ms",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v, 1),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Tucker tensor, generated in-process)",
+        "config": {"workload": "dense 96x96x96x96 FP32 Tucker(16^4) + N(0,1e-6), seed 1, "
+                               "upcast to FP64; reference HOOI_ALS, ranks 16^4"},
+        "cpu_baseline": {"value": round(v, 1), "unit": "ms", "kind": "reference",
+                         "cores": os.cpu_count(),
+                         "sample": f"each step: one HOOI_ALS sweep ({one:.0f} ms median) "
+                                   f"x {sweeps} sweeps to converge"},
+        "e2e": {"value": round(v, 1), "unit": "ms", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-ttmc", dest="ttmc", action="store_false")
+    ap.add_argument("--no-cpu", dest="cpu", action="store_false")
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

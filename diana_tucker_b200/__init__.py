@@ -205,10 +205,35 @@ class Context:
                                        L0.ctypes.data, L0.shape[1], iters, Q.ctypes.data))
         return Q
 
+    def ttm_tc(self, X, U, n: int, split: bool = False):
+        """Y = X x_n U^T on the tensor cores (FP32 in/out, BF16 or hi+lo
+        operands).  U is I_n x J."""
+        self._bind(X, U)
+        X = np.asfortranarray(X, dtype=np.float32)
+        U = np.asfortranarray(U, dtype=np.float64)
+        shape = list(X.shape)
+        J = int(U.shape[1])
+        out_shape = shape.copy()
+        out_shape[n] = J
+        Y = np.zeros(out_shape, dtype=np.float32, order="F")
+        s = _shape_arr(shape)
+        _lib.check(self.lib.dt_ttm_tc(self.h, X.ctypes.data, len(shape), _i64p(s), n,
+                                      U.ctypes.data, J, int(split), Y.ctypes.data))
+        return Y
+
+    def gram_tc(self, Y, split: bool = False):
+        """S = Y Y^T for a row-major I x K FP32 matrix, on the tensor cores."""
+        self._bind(Y)
+        Y = np.ascontiguousarray(Y, dtype=np.float32)
+        I, K = Y.shape
+        S = np.zeros((I, I), order="F")
+        _lib.check(self.lib.dt_gram_tc(self.h, Y.ctypes.data, I, K, int(split), S.ctypes.data))
+        return S
+
     # -- dense HOOI ----------------------------------------------------------
     def hooi_dense(self, X, ranks, *, init="randn", seed=1, U0=None, max_sweeps=5, tol=0.0,
                    inner_iters=5, precision=DT_PREC_FP64, refine_sweeps=0, verbose=False,
-                   want_factors=True, want_core=True):
+                   want_factors=True, want_core=True, profile=False, shape=None):
         """Algorithm::Tucker::HOOI_ALS.  X: numpy or torch (float64/float32),
         column-major.  Returns (G, U, report-dict)."""
         self._bind(X)
@@ -217,7 +242,9 @@ class Context:
             import torch
             dtype = _lib.DT_F64 if X.dtype == torch.float64 else _lib.DT_F32
             xptr = ctypes.c_void_p(X.data_ptr())
-            shape = list(X.shape)
+            # A torch buffer holds the column-major data; pass the tensor
+            # shape explicitly when the buffer is flat.
+            shape = list(shape) if shape is not None else list(X.shape)
         else:
             X = np.asarray(X)
             if X.dtype not in (np.float64, np.float32):
@@ -239,6 +266,7 @@ class Context:
         opts.precision = precision
         opts.refine_sweeps = refine_sweeps
         opts.verbose = int(verbose)
+        opts.profile = int(profile)
         G = np.zeros(ranks, order="F") if want_core else None
         U = ([np.zeros((shape[n], ranks[n]), order="F") for n in range(N)]
              if (want_factors or U0 is not None) else None)

@@ -46,6 +46,7 @@ class HooiOpts(ctypes.Structure):
         ("precision", ctypes.c_int),
         ("refine_sweeps", ctypes.c_int),
         ("verbose", ctypes.c_int),
+        ("profile", ctypes.c_int),
     ]
 
 
@@ -58,6 +59,10 @@ class HooiReport(ctypes.Structure):
         ("device_ms", ctypes.c_double),
         ("res_hist", ctypes.c_double * DT_MAX_HIST),
         ("kernel_launches", ctypes.c_int),
+        ("precision_used", ctypes.c_int),
+        ("ttm_x_launches", ctypes.c_int),
+        ("ttm_x_ms", ctypes.c_double),
+        ("ttm_x_bytes", ctypes.c_double),
     ]
 
     def as_dict(self):
@@ -69,6 +74,10 @@ class HooiReport(ctypes.Structure):
             "device_ms": self.device_ms,
             "res_hist": list(self.res_hist[: min(self.sweeps, DT_MAX_HIST)]),
             "kernel_launches": self.kernel_launches,
+            "precision_used": self.precision_used,
+            "ttm_x_launches": self.ttm_x_launches,
+            "ttm_x_ms": self.ttm_x_ms,
+            "ttm_x_bytes": self.ttm_x_bytes,
         }
 
 
@@ -94,6 +103,9 @@ _SIGS = [
     ("dt_orth2_f64", ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.c_int64]),
     ("dt_als_f64", ctypes.c_int, [_vp, _vp, ctypes.c_int, c_i64p, ctypes.c_int, _vp,
                                   ctypes.c_int64, ctypes.c_int, _vp]),
+    ("dt_ttm_tc", ctypes.c_int, [_vp, _vp, ctypes.c_int, c_i64p, ctypes.c_int, _vp,
+                                 ctypes.c_int64, ctypes.c_int, _vp]),
+    ("dt_gram_tc", ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, _vp]),
     ("dt_hooi_dense", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, c_i64p, c_i64p,
                                      ctypes.POINTER(HooiOpts), _vp, ctypes.POINTER(_vp),
                                      ctypes.POINTER(HooiReport)]),

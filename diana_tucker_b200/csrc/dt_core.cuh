@@ -141,6 +141,49 @@ class DevView {
     DevMem mem_;
 };
 
+// CUDA-event pairs around selected launches (opts.profile), summed at the end.
+class LaunchTimer {
+   public:
+    explicit LaunchTimer(dt_ctx *ctx, bool on) : ctx_(ctx), on_(on) {}
+    ~LaunchTimer() {
+        for (auto &p : ev_) {
+            cudaEventDestroy(p.first);
+            cudaEventDestroy(p.second);
+        }
+    }
+    void begin() {
+        if (!on_) return;
+        cudaEvent_t a, b;
+        DT_CUDA(cudaEventCreate(&a));
+        DT_CUDA(cudaEventCreate(&b));
+        ev_.push_back({a, b});
+        DT_CUDA(cudaEventRecord(a, ctx_->stream));
+    }
+    void end(double bytes) {
+        if (!on_) return;
+        DT_CUDA(cudaEventRecord(ev_.back().second, ctx_->stream));
+        bytes_ += bytes;
+    }
+    // Call after the stream has been synchronised.
+    double total_ms() const {
+        double t = 0.0;
+        for (auto &p : ev_) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, p.first, p.second);
+            t += ms;
+        }
+        return t;
+    }
+    int count() const { return (int)ev_.size(); }
+    double bytes() const { return bytes_; }
+
+   private:
+    dt_ctx *ctx_;
+    bool on_;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_;
+    double bytes_ = 0.0;
+};
+
 inline int64_t prod(const int64_t *s, int n) {
     int64_t p = 1;
     for (int i = 0; i < n; i++) p *= s[i];

@@ -90,6 +90,13 @@ int dt_ctx_create(int device, dt_ctx **out) {
         auto *ctx = new dt_ctx();
         ctx->device = device;
         ctx->num_sms = prop.multiProcessorCount;
+        // Keep freed stream-ordered allocations cached in the device's pool:
+        // with the default threshold of 0 every synchronisation returns them
+        // to the driver and the next cudaMallocAsync has to map pages again.
+        cudaMemPool_t pool;
+        DT_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+        uint64_t keep = ~0ULL;
+        DT_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
         DT_CUDA(cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking));
         ctx->stream = ctx->own_stream;
         DT_CUDA(cudaEventCreate(&ctx->ev_start));

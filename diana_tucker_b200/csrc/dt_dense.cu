@@ -30,13 +30,18 @@ __global__ void __launch_bounds__(TTM_NT) ttm_kernel(const TX *__restrict__ X, i
                                                      int64_t I, int64_t P,
                                                      const double *__restrict__ M, int64_t msj,
                                                      int64_t msi, int64_t J,
-                                                     double *__restrict__ Y) {
+                                                     double *__restrict__ Y, int64_t kchunk,
+                                                     int64_t ysize) {
     __shared__ __align__(16) double Xs[TTM_BK][TTM_BP];
     __shared__ __align__(16) double Ms[TTM_BK][JT];
     const int t = threadIdx.x;
     const int64_t p0 = (int64_t)blockIdx.x * TTM_BP;
     const int64_t j0 = (int64_t)blockIdx.y * JT;
     const int64_t LI = L * I;
+    // Split-K: blockIdx.z owns i in [ibeg, iend) and writes its own partial Y.
+    const int64_t ibeg = (int64_t)blockIdx.z * kchunk;
+    const int64_t iend = min(I, ibeg + kchunk);
+    Y += (int64_t)blockIdx.z * ysize;
 
     // Loader bookkeeping for L > 1: this thread loads rows t and t + 128.
     int64_t lbase[2];
@@ -57,7 +62,7 @@ __global__ void __launch_bounds__(TTM_NT) ttm_kernel(const TX *__restrict__ X, i
 #pragma unroll
         for (int j = 0; j < JT; j++) acc[r][j] = 0.0;
 
-    for (int64_t i0 = 0; i0 < I; i0 += TTM_BK) {
+    for (int64_t i0 = ibeg; i0 < iend; i0 += TTM_BK) {
         if (L > 1) {
 #pragma unroll
             for (int s = 0; s < 2; s++) {
@@ -65,7 +70,7 @@ __global__ void __launch_bounds__(TTM_NT) ttm_kernel(const TX *__restrict__ X, i
 #pragma unroll 4
                 for (int k = 0; k < TTM_BK; k++) {
                     const int64_t i = i0 + k;
-                    Xs[k][pp] = (lok[s] && i < I) ? (double)X[lbase[s] + L * i] : 0.0;
+                    Xs[k][pp] = (lok[s] && i < iend) ? (double)X[lbase[s] + L * i] : 0.0;
                 }
             }
         } else {
@@ -76,13 +81,13 @@ __global__ void __launch_bounds__(TTM_NT) ttm_kernel(const TX *__restrict__ X, i
             for (int s = 0; s < TTM_BP / 8; s++) {
                 const int pp = g + 8 * s;
                 const int64_t p = p0 + pp;
-                Xs[k][pp] = (p < P && i < I) ? (double)X[p * I + i] : 0.0;
+                Xs[k][pp] = (p < P && i < iend) ? (double)X[p * I + i] : 0.0;
             }
         }
         for (int e = t; e < TTM_BK * JT; e += TTM_NT) {
             const int k = e / JT, j = e - (e / JT) * JT;
             const int64_t i = i0 + k, jj = j0 + j;
-            Ms[k][j] = (i < I && jj < J) ? M[jj * msj + i * msi] : 0.0;
+            Ms[k][j] = (i < iend && jj < J) ? M[jj * msj + i * msi] : 0.0;
         }
         __syncthreads();
 #pragma unroll
@@ -113,12 +118,236 @@ __global__ void __launch_bounds__(TTM_NT) ttm_kernel(const TX *__restrict__ X, i
     }
 }
 
+// ---------------------------------------------------------------------------
+// Pipelined TTM for the two layouts the HOOI dimension tree produces from X:
+//   ROWS (L % 256 == 0): the 256 output rows of a CTA are one contiguous run
+//        of l, so every k of a tile is a 16-byte-aligned contiguous segment;
+//   KFAST (L == 1): the contracted index is contiguous, each row of the tile
+//        is 16 consecutive i.
+// Tiles move with cp.async (16 B, zero-filled past I) into a two-stage ring so
+// the next K-chunk streams while this one is multiplied.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(s), "l"(gmem),
+                 "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, int src_bytes) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(s), "l"(gmem),
+                 "r"(src_bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <class TX, int JT, bool KFAST>
+__global__ void __launch_bounds__(TTM_NT) ttm_pipe_kernel(const TX *__restrict__ X, int64_t L,
+                                                          int64_t I, int64_t P,
+                                                          const double *__restrict__ M,
+                                                          int64_t msj, int64_t msi, int64_t J,
+                                                          double *__restrict__ Y, int64_t kchunk,
+                                                          int64_t ysize) {
+    constexpr int EV = 16 / sizeof(TX);              // elements per 16-byte copy
+    constexpr int KROW = 16 + (KFAST ? EV : 0);      // KFAST row stride (elements), padded
+    constexpr int XS_ELEMS = KFAST ? TTM_BP * KROW : TTM_BK * TTM_BP;
+    extern __shared__ __align__(16) uint8_t pipe_smem[];
+    auto Ms = reinterpret_cast<double(*)[TTM_BK][JT]>(pipe_smem);
+    auto Xs = reinterpret_cast<TX(*)[XS_ELEMS]>(pipe_smem + 2 * TTM_BK * JT * sizeof(double));
+    const int t = threadIdx.x;
+    const int64_t p0 = (int64_t)blockIdx.x * TTM_BP;
+    const int64_t j0 = (int64_t)blockIdx.y * JT;
+    const int64_t ibeg = (int64_t)blockIdx.z * kchunk;
+    const int64_t iend = min(I, ibeg + kchunk);
+    Y += (int64_t)blockIdx.z * ysize;
+    const int64_t nch = (iend - ibeg + TTM_BK - 1) / TTM_BK;
+    // ROWS: the CTA's rows are l0..l0+255 of batch b.
+    const int64_t b0 = KFAST ? 0 : p0 / L;
+    const int64_t l0 = KFAST ? 0 : p0 - b0 * L;
+    const TX *xb = KFAST ? X : X + l0 + L * I * b0;
+
+    auto issue = [&](int64_t c, int st) {
+        const int64_t i0 = ibeg + c * TTM_BK;
+        if (!KFAST) {
+            // 16 k x 256 rows: (256 / EV) copies per k.
+            constexpr int PER_K = TTM_BP / EV;
+            for (int e = t; e < TTM_BK * PER_K; e += TTM_NT) {
+                const int k = e / PER_K, q = e - k * PER_K;
+                const int64_t i = i0 + k;
+                const bool ok = i < iend;
+                cp_async16(&Xs[st][k * TTM_BP + q * EV], ok ? xb + L * i + q * EV : X, ok ? 16 : 0);
+            }
+        } else {
+            // 256 rows x 16 i: (16 / EV) copies per row.
+            constexpr int PER_R = TTM_BK / EV;
+            for (int e = t; e < TTM_BP * PER_R; e += TTM_NT) {
+                const int r = e / PER_R, q = e - r * PER_R;
+                const int64_t p = p0 + r, i = i0 + q * EV;
+                const bool ok = p < P && i < iend;
+                cp_async16(&Xs[st][r * KROW + q * EV], ok ? X + p * I + i : X, ok ? 16 : 0);
+            }
+        }
+        for (int e = t; e < TTM_BK * JT; e += TTM_NT) {
+            const int k = e / JT, j = e - k * JT;
+            const int64_t i = i0 + k, jj = j0 + j;
+            const bool ok = i < iend && jj < J;
+            cp_async8(&Ms[st][k][j], ok ? M + jj * msj + i * msi : M, ok ? 8 : 0);
+        }
+        cp_async_commit();
+    };
+
+    double acc[2][JT];
+#pragma unroll
+    for (int r = 0; r < 2; r++)
+#pragma unroll
+        for (int j = 0; j < JT; j++) acc[r][j] = 0.0;
+
+    if (nch > 0) issue(0, 0);
+    for (int64_t c = 0; c < nch; c++) {
+        const int st = (int)(c & 1);
+        if (c + 1 < nch) {
+            issue(c + 1, st ^ 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        if (!KFAST) {
+#pragma unroll
+            for (int k = 0; k < TTM_BK; k++) {
+                double x0, x1;
+                if (sizeof(TX) == 4) {
+                    const float2 v = *reinterpret_cast<const float2 *>(&Xs[st][k * TTM_BP + 2 * t]);
+                    x0 = v.x;
+                    x1 = v.y;
+                } else {
+                    const double2 v = *reinterpret_cast<const double2 *>(&Xs[st][k * TTM_BP + 2 * t]);
+                    x0 = v.x;
+                    x1 = v.y;
+                }
+#pragma unroll
+                for (int j = 0; j < JT; j += 2) {
+                    const double2 m = *reinterpret_cast<const double2 *>(&Ms[st][k][j]);
+                    acc[0][j] = fma(x0, m.x, acc[0][j]);
+                    acc[0][j + 1] = fma(x0, m.y, acc[0][j + 1]);
+                    acc[1][j] = fma(x1, m.x, acc[1][j]);
+                    acc[1][j + 1] = fma(x1, m.y, acc[1][j + 1]);
+                }
+            }
+        } else {
+            // Rows t and t + 128; EV consecutive k per 16-byte shared load.
+#pragma unroll
+            for (int kq = 0; kq < TTM_BK; kq += EV) {
+                double xv[2][EV];
+#pragma unroll
+                for (int r = 0; r < 2; r++) {
+                    const TX *src = &Xs[st][(t + r * TTM_NT) * KROW + kq];
+                    if (sizeof(TX) == 4) {
+                        const float4 v = *reinterpret_cast<const float4 *>(src);
+                        const float f[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                        for (int q = 0; q < EV; q++) xv[r][q] = f[q];
+                    } else {
+                        const double2 v = *reinterpret_cast<const double2 *>(src);
+                        const double f[2] = {v.x, v.y};
+#pragma unroll
+                        for (int q = 0; q < EV; q++) xv[r][q] = f[q];
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < EV; q++) {
+#pragma unroll
+                    for (int j = 0; j < JT; j += 2) {
+                        const double2 m = *reinterpret_cast<const double2 *>(&Ms[st][kq + q][j]);
+                        acc[0][j] = fma(xv[0][q], m.x, acc[0][j]);
+                        acc[0][j + 1] = fma(xv[0][q], m.y, acc[0][j + 1]);
+                        acc[1][j] = fma(xv[1][q], m.x, acc[1][j]);
+                        acc[1][j + 1] = fma(xv[1][q], m.y, acc[1][j + 1]);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+
+    const int64_t LJ = L * J;
+#pragma unroll
+    for (int r = 0; r < 2; r++) {
+        const int64_t p = KFAST ? p0 + t + r * TTM_NT : p0 + 2 * t + r;
+        if (p >= P) continue;
+        const int64_t b = p / L, l = p - b * L;
+        double *y = Y + l + LJ * b;
+#pragma unroll
+        for (int j = 0; j < JT; j++)
+            if (j0 + j < J) y[L * (j0 + j)] = acc[r][j];
+    }
+}
+
+__global__ void sum_splits_kernel(const double *__restrict__ part, int nsplit, int64_t n,
+                                  double *__restrict__ out) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int z = 0; z < nsplit; z++) s += part[z * n + e];
+        out[e] = s;
+    }
+}
+
 template <class TX, int JT>
 void ttm_launch(dt_ctx *ctx, const TX *X, int64_t L, int64_t I, int64_t B, const double *M,
                 int64_t msj, int64_t msi, int64_t J, double *Y) {
     const int64_t P = L * B;
-    dim3 grid(ceil_div(P, TTM_BP), ceil_div(J, JT));
-    DT_LAUNCH(ctx, (ttm_kernel<TX, JT>), grid, TTM_NT, 0, X, L, I, P, M, msj, msi, J, Y);
+    const int64_t base = (int64_t)ceil_div(P, TTM_BP) * ceil_div(J, JT);
+    // Few output rows: split the contraction so the GPU has enough CTAs, and
+    // sum the partial outputs in a fixed order (deterministic).
+    int64_t nsplit = 1;
+    const int64_t target = 4LL * ctx->num_sms;
+    if (base < target && I >= 64) {
+        nsplit = std::min<int64_t>((target + base - 1) / base, I / 32);
+        nsplit = std::max<int64_t>(nsplit, 1);
+    }
+    int64_t kchunk = ((I + nsplit - 1) / nsplit + TTM_BK - 1) / TTM_BK * TTM_BK;
+    nsplit = (I + kchunk - 1) / kchunk;
+    const int64_t ysize = P * J;
+    dim3 grid(ceil_div(P, TTM_BP), ceil_div(J, JT), (unsigned)nsplit);
+    const uintptr_t xa = reinterpret_cast<uintptr_t>(X);
+    const bool rows_ok = L % TTM_BP == 0 && xa % 16 == 0;
+    const bool kfast_ok = L == 1 && (I * sizeof(TX)) % 16 == 0 && xa % 16 == 0 &&
+                          (kchunk * sizeof(TX)) % 16 == 0;
+    constexpr int EV = 16 / sizeof(TX);
+    const size_t smem_rows = 2 * TTM_BK * JT * sizeof(double) + 2 * TTM_BK * TTM_BP * sizeof(TX);
+    const size_t smem_kfast =
+        2 * TTM_BK * JT * sizeof(double) + 2 * TTM_BP * (TTM_BK + EV) * sizeof(TX);
+    auto launch = [&](double *dst) {
+        if (rows_ok) {
+            DT_CUDA(cudaFuncSetAttribute(ttm_pipe_kernel<TX, JT, false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem_rows));
+            DT_LAUNCH(ctx, (ttm_pipe_kernel<TX, JT, false>), grid, TTM_NT, smem_rows, X, L, I, P,
+                      M, msj, msi, J, dst, kchunk, ysize);
+        } else if (kfast_ok) {
+            DT_CUDA(cudaFuncSetAttribute(ttm_pipe_kernel<TX, JT, true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem_kfast));
+            DT_LAUNCH(ctx, (ttm_pipe_kernel<TX, JT, true>), grid, TTM_NT, smem_kfast, X, L, I, P,
+                      M, msj, msi, J, dst, kchunk, ysize);
+        }
+        else
+            DT_LAUNCH(ctx, (ttm_kernel<TX, JT>), grid, TTM_NT, 0, X, L, I, P, M, msj, msi, J, dst,
+                      kchunk, ysize);
+    };
+    if (nsplit == 1) {
+        launch(Y);
+        return;
+    }
+    DevMem part(ctx, (size_t)nsplit * ysize * sizeof(double));
+    launch(part.as<double>());
+    const unsigned blocks = std::max(1u, std::min<unsigned>(ceil_div(ysize, 256), 8u * ctx->num_sms));
+    DT_LAUNCH(ctx, sum_splits_kernel, blocks, 256, 0, part.as<double>(), (int)nsplit, ysize, Y);
 }
 
 }  // namespace

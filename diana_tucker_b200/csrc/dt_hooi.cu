@@ -99,12 +99,17 @@ DevMem DenseHooi::contract(const void *t, int tdtype, int64_t *shape, int m) {
     for (int k = 0; k < m; k++) L *= shape[k];
     for (int k = m + 1; k < N; k++) B *= shape[k];
     DevMem out(ctx, L * R[m] * B * sizeof(double));
+    const bool from_x = xtimer && t == Xdev;
+    if (from_x) xtimer->begin();
     if (tdtype == DT_F32)
         ttm_f64<float>(ctx, static_cast<const float *>(t), L, shape[m], B, U[m].as<double>(),
                        I[m], 1, R[m], out.as<double>());
     else
         ttm_f64<double>(ctx, static_cast<const double *>(t), L, shape[m], B,
                         U[m].as<double>(), I[m], 1, R[m], out.as<double>());
+    if (from_x)
+        xtimer->end((double)L * shape[m] * B * (tdtype == DT_F32 ? 4 : 8) +
+                    (double)L * R[m] * B * 8 + (double)I[m] * R[m] * 8);
     shape[m] = R[m];
     return out;
 }
@@ -231,6 +236,8 @@ double DenseHooi::read_scalar(int k) {
 
 void DenseHooi::run(double *G_user, double *const *U_user, dt_hooi_report *rep) {
     const int64_t launches0 = ctx->launches;
+    LaunchTimer timer(ctx, opts.profile != 0);
+    xtimer = &timer;
     DT_CUDA(cudaEventRecord(ctx->ev_start, ctx->stream));
     sumsq(ctx, Xdev, dtype, xsize, scal.as<double>());
     init_factors(U_user);
@@ -289,7 +296,12 @@ void DenseHooi::run(double *G_user, double *const *U_user, dt_hooi_report *rep) 
         rep->residual = std::sqrt(std::max(0.0, 1.0 - g2 / x2));
         rep->device_ms = ms;
         rep->kernel_launches = (int)(ctx->launches - launches0);
+        rep->precision_used = DT_PREC_FP64;
+        rep->ttm_x_launches = timer.count();
+        rep->ttm_x_ms = timer.total_ms();
+        rep->ttm_x_bytes = timer.bytes();
     }
+    xtimer = nullptr;
 }
 
 }  // namespace dt

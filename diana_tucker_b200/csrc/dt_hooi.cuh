@@ -22,6 +22,7 @@ struct DenseHooi {
     std::vector<DevMem> U;    // I_n x R_n col-major
     DevMem S, work, flag, scal, G;
     int hosvd_iters = 30;
+    LaunchTimer *xtimer = nullptr;  // times the TTM launches that read X
 
     void setup(dt_ctx *c, const void *X, int dtype, int n, const int64_t *shape,
                const int64_t *ranks, const dt_hooi_opts &o);

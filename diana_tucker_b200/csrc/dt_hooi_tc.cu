@@ -1,15 +1,401 @@
-// Mixed-precision dense HOOI on the tcgen05 tensor cores.
+// Mixed-precision dense HOOI: the TTM chain and the Gram run on the tcgen05
+// tensor cores in BF16 (optionally with hi+lo split operands) with FP32
+// accumulation; the subspace iteration / QR, the fit subtraction and the
+// final core projection stay in FP64.
+//
+// Schedule: sweeps in plain BF16 until the residual settles to the BF16 noise
+// floor, then `refine_sweeps` sweeps with split hi+lo operands (~2^-16
+// relative), then the core G = X x_1 U_1^T ... x_N U_N^T projected in FP64 from
+// the original X.  DT_PREC_BF16X2 runs every sweep split.  The same dimension
+// tree as the FP64 driver is used; each chain contracts its highest mode
+// first so the non-contracted prefix (the TMA row dimension) stays long, and a
+// leaf's last contraction writes Y_(n) K-major for the Gram.
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
 #include "dt_hooi.cuh"
 #include "dt_kernels.cuh"
+#include "dt_tc_host.cuh"
 
 namespace dt {
+namespace {
+
+__global__ void f64_to_f32_kernel(const double *__restrict__ x, int64_t n, float *__restrict__ y) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
+         e += (int64_t)gridDim.x * blockDim.x)
+        y[e] = (float)x[e];
+}
+
+struct BfTensor {
+    DevMem hi, lo;
+    int64_t shape[16];
+};
+
+struct MixedHooi {
+    dt_ctx *ctx = nullptr;
+    int N = 0;
+    int64_t I[16] = {}, R[16] = {};
+    int64_t xsize = 0;
+    dt_hooi_opts opts{};
+    const float *X32 = nullptr;
+    DevMem X32own, Xh, Xl;
+    std::vector<DevMem> U;
+    DevMem S, work, flag, err, scal, Gs;
+    bool split = false;
+    DenseHooi helper;  // initial factors (same generators as the FP64 driver)
+    LaunchTimer *xtimer = nullptr;
+
+    static std::vector<int> order_high_first(std::vector<int> modes) {
+        std::sort(modes.begin(), modes.end(), [](int a, int b) { return a > b; });
+        return modes;
+    }
+
+    // Checks every contraction and Gram of the dimension tree against the
+    // tensor-core kernels' layout rules.
+    bool plan_ok() const {
+        if (N < 2 || N > 8) return false;
+        for (int n = 0; n < N; n++) {
+            int64_t K = 1;
+            for (int m = 0; m < N; m++)
+                if (m != n) K *= R[m];
+            if (!tc_gram_supported(I[n], K) || R[n] > 32) return false;
+        }
+        std::vector<int64_t> sh(I, I + N);
+        return node_ok(0, N, sh);
+    }
+    bool node_ok(int lo, int hi, std::vector<int64_t> sh) const {
+        if (hi - lo == 1) return true;
+        const int mid = (lo + hi + 1) / 2;  // [0,3) -> [0,2) + [2,3): long TMA rows
+        for (int side = 0; side < 2; side++) {
+            const int clo = side == 0 ? lo : mid, chi = side == 0 ? mid : hi;
+            std::vector<int> modes;
+            for (int m = lo; m < hi; m++)
+                if (m < clo || m >= chi) modes.push_back(m);
+            std::vector<int64_t> c = sh;
+            for (int m : order_high_first(modes)) {
+                int64_t L = 1, B = 1;
+                for (int k = 0; k < m; k++) L *= c[k];
+                for (int k = m + 1; k < N; k++) B *= c[k];
+                if (!tc_ttm_supported(L, c[m], B, R[m])) return false;
+                c[m] = R[m];
+            }
+            if (!node_ok(clo, chi, c)) return false;
+        }
+        return true;
+    }
+
+    // Contract `modes` of T; the last contraction of a leaf chain (leaf >= 0)
+    // writes Y_(leaf) K-major.
+    BfTensor contract_all(const __nv_bfloat16 *Th, const __nv_bfloat16 *Tl,
+                          const int64_t *shape, std::vector<int> modes, int leaf) {
+        BfTensor cur;
+        std::memcpy(cur.shape, shape, N * sizeof(int64_t));
+        const __nv_bfloat16 *sh = Th, *sl = Tl;
+        const std::vector<int> ord = order_high_first(modes);
+        for (size_t q = 0; q < ord.size(); q++) {
+            const int m = ord[q];
+            int64_t L = 1, B = 1;
+            for (int k = 0; k < m; k++) L *= cur.shape[k];
+            for (int k = m + 1; k < N; k++) B *= cur.shape[k];
+            const int64_t outn = L * R[m] * B;
+            BfTensor nxt;
+            std::memcpy(nxt.shape, cur.shape, N * sizeof(int64_t));
+            nxt.shape[m] = R[m];
+            nxt.hi.alloc(ctx, outn * sizeof(__nv_bfloat16));
+            if (split) nxt.lo.alloc(ctx, outn * sizeof(__nv_bfloat16));
+            OutMap om;
+            const bool last_of_leaf = leaf >= 0 && q + 1 == ord.size();
+            if (!last_of_leaf) {
+                om.nl = 1;
+                om.dl[0] = std::max<int64_t>(L, 1);
+                om.sl[0] = 1;
+                om.nb = 1;
+                om.db[0] = std::max<int64_t>(B, 1);
+                om.sb[0] = L * R[m];
+                om.jstride = L;
+            } else {
+                // Y_(leaf)[t_leaf][k], k = sum_{q != leaf} t_q * kst_q.
+                int64_t kst[16], K = 1;
+                for (int p = 0; p < N; p++) {
+                    if (p == leaf) continue;
+                    kst[p] = K;
+                    K *= nxt.shape[p];
+                }
+                kst[leaf] = K;
+                om.nl = m;
+                for (int p = 0; p < m; p++) {
+                    om.dl[p] = cur.shape[p];
+                    om.sl[p] = kst[p];
+                }
+                om.nb = N - m - 1;
+                for (int p = m + 1; p < N; p++) {
+                    om.db[p - m - 1] = cur.shape[p];
+                    om.sb[p - m - 1] = kst[p];
+                }
+                om.jstride = kst[m];
+                if (om.nl == 0) {
+                    om.nl = 1;
+                    om.dl[0] = 1;
+                    om.sl[0] = 0;
+                }
+                if (om.nb == 0) {
+                    om.nb = 1;
+                    om.db[0] = 1;
+                    om.sb[0] = 0;
+                }
+            }
+            const bool from_x = xtimer && sh == Xh.as<__nv_bfloat16>();
+            if (from_x) xtimer->begin();
+            tc_ttm(ctx, sh, split ? sl : nullptr, L, cur.shape[m], B, U[m].as<double>(), R[m], om,
+                   nxt.hi.as<__nv_bfloat16>(), split ? nxt.lo.as<__nv_bfloat16>() : nullptr,
+                   nullptr, err.as<int>());
+            if (from_x)
+                xtimer->end(((double)L * cur.shape[m] * B + (double)L * R[m] * B) * 2 *
+                                (split ? 2 : 1) +
+                            (double)cur.shape[m] * R[m] * 8);
+            cur = std::move(nxt);
+            sh = cur.hi.as<__nv_bfloat16>();
+            sl = split ? cur.lo.as<__nv_bfloat16>() : nullptr;
+        }
+        return cur;
+    }
+
+    void leaf(int n, const BfTensor &Y) {
+        int64_t K = 1;
+        for (int m = 0; m < N; m++)
+            if (m != n) K *= R[m];
+        const __nv_bfloat16 *yh = Y.hi.as<__nv_bfloat16>();
+        const __nv_bfloat16 *yl = split ? Y.lo.as<__nv_bfloat16>() : nullptr;
+        tc_gram(ctx, yh, yl, I[n], K, S.as<double>(), err.as<int>());
+        subspace_iter(ctx, S.as<double>(), I[n], U[n].as<double>(), R[n], opts.inner_iters,
+                      work.as<double>(), flag.as<int>());
+        if (n == N - 1)
+            core_rows(ctx, yh, yl, I[n], K, U[n].as<double>(), R[n], Gs.as<double>(),
+                      scal.as<double>() + 1);
+    }
+
+    void node(int lo, int hi, const __nv_bfloat16 *Th, const __nv_bfloat16 *Tl,
+              const int64_t *shape) {
+        const int mid = (lo + hi + 1) / 2;  // [0,3) -> [0,2) + [2,3): long TMA rows
+        for (int side = 0; side < 2; side++) {
+            const int clo = side == 0 ? lo : mid, chi = side == 0 ? mid : hi;
+            std::vector<int> modes;
+            for (int m = lo; m < hi; m++)
+                if (m < clo || m >= chi) modes.push_back(m);
+            const bool is_leaf = chi - clo == 1;
+            BfTensor child = contract_all(Th, Tl, shape, modes, is_leaf ? clo : -1);
+            if (is_leaf)
+                leaf(clo, child);
+            else
+                node(clo, chi, child.hi.as<__nv_bfloat16>(),
+                     split ? child.lo.as<__nv_bfloat16>() : nullptr, child.shape);
+        }
+    }
+
+    void sweep() {
+        node(0, N, Xh.as<__nv_bfloat16>(), split ? Xl.as<__nv_bfloat16>() : nullptr, I);
+    }
+
+    double read_scalar(int k) {
+        double h = 0.0;
+        DT_CUDA(cudaMemcpyAsync(&h, scal.as<double>() + k, sizeof(double), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+        DT_CUDA(cudaStreamSynchronize(ctx->stream));
+        return h;
+    }
+
+    void run(const void *X, int dtype, double *G_user, double *const *U_user,
+             dt_hooi_report *rep) {
+        const int64_t launches0 = ctx->launches;
+        LaunchTimer timer(ctx, opts.profile != 0);
+        xtimer = &timer;
+        const bool want_split =
+            opts.precision == DT_PREC_BF16X2 || opts.refine_sweeps > 0;
+        DT_CUDA(cudaEventRecord(ctx->ev_start, ctx->stream));
+        if (dtype == DT_F32) {
+            X32 = static_cast<const float *>(X);
+        } else {
+            X32own.alloc(ctx, xsize * sizeof(float));
+            const unsigned blocks = std::max(1u, std::min<unsigned>(ceil_div(xsize, 256), 8u * ctx->num_sms));
+            DT_LAUNCH(ctx, f64_to_f32_kernel, blocks, 256, 0, static_cast<const double *>(X), xsize,
+                      X32own.as<float>());
+            X32 = X32own.as<float>();
+        }
+        Xh.alloc(ctx, xsize * sizeof(__nv_bfloat16));
+        if (want_split) Xl.alloc(ctx, xsize * sizeof(__nv_bfloat16));
+        if (dtype == DT_F64)
+            sumsq(ctx, X, DT_F64, xsize, scal.as<double>());
+        DevMem x2f(ctx, sizeof(double));
+        split_f32(ctx, X32, xsize, Xh.as<__nv_bfloat16>(),
+                  want_split ? Xl.as<__nv_bfloat16>() : nullptr,
+                  dtype == DT_F32 ? scal.as<double>() : x2f.as<double>());
+        // Initial factors: the FP64 driver's generators (libc Gaussian + QR,
+        // or the caller's); HOSVD is not offered on this path.
+        helper.init_factors(U_user);
+        for (int m = 0; m < N; m++)
+            DT_CUDA(cudaMemcpyAsync(U[m].get(), helper.U[m].get(), I[m] * R[m] * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, ctx->stream));
+        const double x2 = read_scalar(0);
+        // Phases: BF16 sweeps until the residual settles to the BF16 noise
+        // floor (kBf16Settle) or kBf16Max sweeps, then split hi+lo sweeps:
+        // `refine_sweeps` of them (DT_PREC_BF16), or until the residual
+        // settles to max(tol, kSplitFloor) (DT_PREC_BF16X2).  The residual a
+        // sweep tracks comes from its own low-precision core, so the floors
+        // sit above that noise; the reported residual is the FP64 projection.
+        constexpr double kBf16Settle = 1e-3, kSplitFloor = 5e-6;
+        constexpr int kBf16Max = 8;
+        double prev = -1.0, res = 0.0;
+        int sweeps = 0, bf16_done = 0, split_done = 0;
+        const bool refine_mode = opts.precision == DT_PREC_BF16;
+        split = opts.precision == DT_PREC_BF16X2;
+        for (int it = 0; it < opts.max_sweeps; it++) {
+            if (!split && refine_mode && opts.refine_sweeps > 0 &&
+                it >= opts.max_sweeps - opts.refine_sweeps) {
+                split = true;
+                prev = -1.0;
+            }
+            sweep();
+            const double g2 = read_scalar(1);
+            res = std::sqrt(std::max(0.0, 1.0 - g2 / x2));
+            if (rep && it < DT_MAX_HIST) rep->res_hist[it] = res;
+            sweeps = it + 1;
+            if (opts.verbose)
+                fprintf(stderr, "[dt_hooi bf16%s] sweep %d  residual = %.12e\n", split ? "x2" : "",
+                        it + 1, res);
+            const double delta = prev >= 0 ? std::fabs(res - prev) : 1e300;
+            prev = res;
+            if (!split) {
+                bf16_done++;
+                const bool settled = delta < kBf16Settle || bf16_done >= kBf16Max;
+                if (opts.refine_sweeps > 0 && settled) {
+                    split = true;
+                    prev = -1.0;
+                } else if (opts.refine_sweeps == 0 && opts.tol > 0 && delta < std::max(opts.tol, kBf16Settle)) {
+                    break;
+                }
+            } else {
+                split_done++;
+                if (refine_mode) {
+                    if (split_done >= opts.refine_sweeps) break;
+                    if (opts.tol > 0 && delta < std::max(opts.tol, kSplitFloor)) break;
+                } else if (opts.tol > 0 && delta < std::max(opts.tol, kSplitFloor)) {
+                    break;
+                }
+            }
+        }
+        // Final core, FP64 projection from the original X.
+        int64_t shape[16];
+        std::memcpy(shape, I, N * sizeof(int64_t));
+        std::vector<int> ord(N);
+        std::iota(ord.begin(), ord.end(), 0);
+        std::sort(ord.begin(), ord.end(), [](int a, int b) { return a > b; });
+        DevMem cur;
+        const void *src = X32;
+        bool src_f32 = true;
+        for (int m : ord) {
+            int64_t L = 1, B = 1;
+            for (int k = 0; k < m; k++) L *= shape[k];
+            for (int k = m + 1; k < N; k++) B *= shape[k];
+            DevMem nxt(ctx, L * R[m] * B * sizeof(double));
+            if (src_f32)
+                ttm_f64<float>(ctx, static_cast<const float *>(src), L, shape[m], B,
+                               U[m].as<double>(), I[m], 1, R[m], nxt.as<double>());
+            else
+                ttm_f64<double>(ctx, static_cast<const double *>(src), L, shape[m], B,
+                                U[m].as<double>(), I[m], 1, R[m], nxt.as<double>());
+            shape[m] = R[m];
+            cur = std::move(nxt);
+            src = cur.get();
+            src_f32 = false;
+        }
+        sumsq(ctx, cur.get(), DT_F64, prod(R, N), scal.as<double>() + 2);
+        DT_CUDA(cudaEventRecord(ctx->ev_stop, ctx->stream));
+        const double g2 = read_scalar(2);
+        int herr = 0;
+        DT_CUDA(cudaMemcpyAsync(&herr, err.get(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        DT_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (herr) fail(DT_ERR_CUDA, fmt("tensor-core kernel reported error %d (wait timed out)", herr));
+        float ms = 0.f;
+        DT_CUDA(cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop));
+        if (!std::isfinite(g2)) fail(DT_ERR_NUMERIC, "HOOI produced a non-finite core");
+        if (G_user) {
+            DevView g(ctx, G_user, prod(R, N) * sizeof(double), false, true);
+            DT_CUDA(cudaMemcpyAsync(g.ptr(), cur.get(), prod(R, N) * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, ctx->stream));
+            g.finish();
+        }
+        if (U_user) {
+            for (int m = 0; m < N; m++) {
+                if (!U_user[m]) continue;
+                DevView u(ctx, U_user[m], I[m] * R[m] * sizeof(double), false, true);
+                DT_CUDA(cudaMemcpyAsync(u.ptr(), U[m].get(), I[m] * R[m] * sizeof(double),
+                                        cudaMemcpyDeviceToDevice, ctx->stream));
+                u.finish();
+            }
+        }
+        DT_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (rep) {
+            rep->sweeps = sweeps;
+            rep->x_norm = std::sqrt(x2);
+            rep->g_norm = std::sqrt(g2);
+            rep->residual = std::sqrt(std::max(0.0, 1.0 - g2 / x2));
+            rep->device_ms = ms;
+            rep->kernel_launches = (int)(ctx->launches - launches0);
+            rep->precision_used = opts.precision;
+            rep->ttm_x_launches = timer.count();
+            rep->ttm_x_ms = timer.total_ms();
+            rep->ttm_x_bytes = timer.bytes();
+        }
+        xtimer = nullptr;
+    }
+};
+
+}  // namespace
 
 void hooi_dense_lowprec(dt_ctx *ctx, const void *X, int dtype, int ndim, const int64_t *shape,
                         const int64_t *ranks, const dt_hooi_opts &opts, double *G,
                         double *const *U, dt_hooi_report *report) {
-    (void)ctx; (void)X; (void)dtype; (void)ndim; (void)shape; (void)ranks; (void)opts;
-    (void)G; (void)U; (void)report;
-    fail(DT_ERR_UNSUPPORTED, "tensor-core HOOI not built yet");
+    DT_CHECK_ARG(opts.precision == DT_PREC_BF16 || opts.precision == DT_PREC_BF16X2,
+                 "unknown precision %d", opts.precision);
+    DT_CHECK_ARG(opts.init != DT_INIT_HOSVD,
+                 "the tensor-core HOOI starts from random or given factors, not HOSVD");
+    MixedHooi h;
+    h.ctx = ctx;
+    h.N = ndim;
+    h.opts = opts;
+    for (int m = 0; m < ndim; m++) {
+        h.I[m] = shape[m];
+        h.R[m] = ranks[m];
+    }
+    h.xsize = prod(shape, ndim);
+    if (!h.plan_ok()) {
+        // A shape outside the TMA / UMMA layout rules: run the FP64 engine.
+        dt_hooi_opts o = opts;
+        o.precision = DT_PREC_FP64;
+        DenseHooi f;
+        f.setup(ctx, X, dtype, ndim, shape, ranks, o);
+        f.run(G, U, report);
+        if (report) report->precision_used = DT_PREC_FP64;
+        return;
+    }
+    h.helper.setup(ctx, X, dtype, ndim, shape, ranks, opts);
+    h.U.resize(ndim);
+    int64_t maxI = 0, maxR = 0;
+    for (int m = 0; m < ndim; m++) {
+        h.U[m].alloc(ctx, shape[m] * ranks[m] * sizeof(double));
+        maxI = std::max(maxI, shape[m]);
+        maxR = std::max(maxR, ranks[m]);
+    }
+    h.S.alloc(ctx, maxI * maxI * sizeof(double));
+    h.work.alloc(ctx, (3 * maxI * maxR + maxR + 64) * sizeof(double));
+    h.flag.alloc(ctx, sizeof(int));
+    h.err.alloc(ctx, sizeof(int));
+    h.scal.alloc(ctx, 4 * sizeof(double));
+    h.Gs.alloc(ctx, prod(ranks, ndim) * sizeof(double));
+    DT_CUDA(cudaMemsetAsync(h.flag.get(), 0, sizeof(int), ctx->stream));
+    DT_CUDA(cudaMemsetAsync(h.err.get(), 0, sizeof(int), ctx->stream));
+    h.run(X, dtype, G, U, report);
 }
 
 }  // namespace dt

@@ -118,47 +118,84 @@ __global__ void __launch_bounds__(LA_NT) hqr_kernel(const double *A, int64_t m, 
 }
 
 // Cholesky G = R^T R of the r x r SPD matrix in smem (row-major G[i*r+c]) by
-// one warp, then Rinv = R^{-1} (upper, row-major).  Returns false on a
-// non-positive pivot.  Runs in warp 0 only.
+// one warp, then Rinv = R^{-1} (upper, row-major).  Lane c keeps column c in
+// registers and rows are exchanged with shuffles, so the r pivots form one
+// short dependency chain (one sqrt and one reciprocal per pivot).  Returns
+// false on a non-positive pivot.  Runs in warp 0 only; r <= 32.
+template <int RMAX>
 __device__ bool warp_chol_inv(double *G, double *Rinv, int r) {
     const int lane = threadIdx.x & 31;
+    double g[RMAX], x[RMAX], invd[RMAX];
+#pragma unroll
+    for (int i = 0; i < RMAX; i++) g[i] = (i < r && lane < r) ? G[i * r + lane] : 0.0;
+    const double g00 = __shfl_sync(0xffffffffu, g[0], 0);
     bool ok = true;
-    const double g00 = G[0];
-    for (int k = 0; k < r; k++) {
-        const double d = G[k * r + k];
+#pragma unroll
+    for (int k = 0; k < RMAX; k++) {
+        if (k >= r) break;
+        const double d = __shfl_sync(0xffffffffu, g[k], k);
         if (!(d > 1e-28 * g00)) ok = false;
         const double rkk = sqrt(fmax(d, 1e-300));
-        __syncwarp();
-        for (int c = k + 1 + lane; c < r; c += 32) G[k * r + c] /= rkk;
-        __syncwarp();
-        if (lane == 0) G[k * r + k] = rkk;
-        for (int i = k + 1; i < r; i++) {
-            const double rki = G[k * r + i];
-            for (int c = i + lane; c < r; c += 32) G[i * r + c] = fma(-rki, G[k * r + c], G[i * r + c]);
+        const double inv = 1.0 / rkk;
+        invd[k] = inv;
+        if (lane > k) g[k] *= inv;
+        if (lane == k) g[k] = rkk;
+#pragma unroll
+        for (int i = k + 1; i < RMAX; i++) {
+            if (i >= r) break;
+            const double rki = __shfl_sync(0xffffffffu, g[k], i);
+            if (lane >= i) g[i] = fma(-rki, g[k], g[i]);
         }
-        __syncwarp();
     }
-    // Column c of R^{-1}: back substitution, one lane per column.
-    for (int c = lane; c < r; c += 32) {
-        for (int i = 0; i < r; i++) Rinv[i * r + c] = 0.0;
-        Rinv[c * r + c] = 1.0 / G[c * r + c];
-        for (int i = c - 1; i >= 0; i--) {
-            double s = 0.0;
-            for (int j = i + 1; j <= c; j++) s = fma(G[i * r + j], Rinv[j * r + c], s);
-            Rinv[i * r + c] = -s / G[i * r + i];
+    // Column `lane` of R^{-1} by back substitution; x[j] = 0 for j > lane.
+#pragma unroll
+    for (int i = 0; i < RMAX; i++) x[i] = (i == lane) ? invd[i] : 0.0;
+#pragma unroll
+    for (int i = RMAX - 2; i >= 0; i--) {
+        if (i >= r - 1) continue;
+        double sacc = 0.0;
+#pragma unroll
+        for (int j = i + 1; j < RMAX; j++) {
+            if (j >= r) break;
+            const double rij = __shfl_sync(0xffffffffu, g[i], j);
+            sacc = fma(rij, x[j], sacc);
         }
+        if (i < lane) x[i] = -sacc * invd[i];
+    }
+    if (lane < r) {
+#pragma unroll
+        for (int i = 0; i < RMAX; i++)
+            if (i < r) {
+                Rinv[i * r + lane] = x[i];
+                G[i * r + lane] = i <= lane ? g[i] : 0.0;
+            }
     }
     __syncwarp();
     return ok;
 }
 
 // Subspace iteration L <- orth(S L), `iters` times, one CTA.  S (n x n,
-// symmetric), L and Z (n x r) live in shared memory when they fit, else in
-// the global workspace.  Each step orthonormalises with CholeskyQR2; a
-// Cholesky breakdown (rank-deficient S L) switches that step to Householder.
+// symmetric) is staged in shared memory -- whole when it fits, as its packed
+// upper triangle for n up to ~220, else read from L2.  L and Z (n x r) live in
+// shared memory when they fit.  Intermediate steps orthonormalise with one
+// CholeskyQR pass (only conditioning matters there), the last step with two
+// (CholeskyQR2, orthonormal to FP64 rounding); a Cholesky breakdown
+// (rank-deficient S L) switches that step to Householder.
+enum { S_GLOBAL = 0, S_FULL = 1, S_PACKED = 2 };
+
+__device__ __forceinline__ double s_at(const double *S, int64_t n, int mode, int64_t i,
+                                       int64_t k) {
+    if (mode == S_PACKED) {
+        const int64_t a = i < k ? i : k, b = i < k ? k : i;
+        return S[a + b * (b + 1) / 2];
+    }
+    return S[i + n * k];
+}
+
+template <int RMAX>
 __global__ void __launch_bounds__(LA_NT) subspace_kernel(const double *Sg, int64_t n,
                                                          double *Lg, int64_t r, int iters,
-                                                         double *work, int s_in_smem,
+                                                         double *work, int s_mode,
                                                          int zl_in_smem, int *flag) {
     extern __shared__ __align__(16) double sm[];
     __shared__ double red[33];
@@ -168,11 +205,20 @@ __global__ void __launch_bounds__(LA_NT) subspace_kernel(const double *Sg, int64
     double *Ri = sm + r * r;       // r*r
     double *cur = sm + 2 * r * r;  // after the two r x r blocks
     const double *S = Sg;
-    if (s_in_smem) {
+    if (s_mode == S_FULL) {
         double *Ss = cur;
         for (int64_t e = t; e < n * n; e += blockDim.x) Ss[e] = Sg[e];
         S = Ss;
         cur += n * n;
+    } else if (s_mode == S_PACKED) {
+        double *Ss = cur;
+        const int64_t np = n * (n + 1) / 2;
+        for (int64_t e = t; e < n * n; e += blockDim.x) {
+            const int64_t i = e % n, k = e / n;
+            if (i <= k) Ss[i + k * (k + 1) / 2] = Sg[e];
+        }
+        S = Ss;
+        cur += (np + 1) & ~int64_t(1);
     }
     double *L, *Z;
     if (zl_in_smem) {
@@ -185,33 +231,61 @@ __global__ void __launch_bounds__(LA_NT) subspace_kernel(const double *Sg, int64
     double *hwork = work + 2 * n * r;  // n*r + r for the Householder fallback
     for (int64_t e = t; e < n * r; e += blockDim.x) L[e] = Lg[e];
     __syncthreads();
+    const int64_t cgroups = (r + 3) / 4;
+    const int npairs = (int)(r * (r + 1) / 2);
     for (int it = 0; it < iters; it++) {
-        // Z = S L
-        for (int64_t e = t; e < n * r; e += blockDim.x) {
-            const int64_t i = e % n, c = e / n;
-            const double *lc = L + c * n;
-            double s = 0.0;
-            for (int64_t k = 0; k < n; k++) s = fma(S[i + n * k], lc[k], s);
-            Z[e] = s;
+        // Z = S L; each task is one row i and four columns.
+        for (int64_t task = t; task < n * cgroups; task += blockDim.x) {
+            const int64_t i = task % n, c0 = 4 * (task / n);
+            double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+            const double *l0 = L + c0 * n;
+            const bool h1 = c0 + 1 < r, h2 = c0 + 2 < r, h3 = c0 + 3 < r;
+#pragma unroll 4
+            for (int64_t k = 0; k < n; k++) {
+                const double sv = s_at(S, n, s_mode, i, k);
+                a0 = fma(sv, l0[k], a0);
+                if (h1) a1 = fma(sv, l0[k + n], a1);
+                if (h2) a2 = fma(sv, l0[k + 2 * n], a2);
+                if (h3) a3 = fma(sv, l0[k + 3 * n], a3);
+            }
+            Z[i + c0 * n] = a0;
+            if (h1) Z[i + (c0 + 1) * n] = a1;
+            if (h2) Z[i + (c0 + 2) * n] = a2;
+            if (h3) Z[i + (c0 + 3) * n] = a3;
         }
         __syncthreads();
-        // Two CholeskyQR passes: Z -> L -> Z, final basis copied to L.
         bool broke = false;
-        for (int pass = 0; pass < 2 && !broke; pass++) {
+        const int passes = (it == iters - 1) ? 2 : 1;
+        for (int pass = 0; pass < passes && !broke; pass++) {
             double *src = pass == 0 ? Z : L;
             double *dst = pass == 0 ? L : Z;
-            for (int e = t; e < r * r; e += blockDim.x) {
-                const int a = e / (int)r, b = e % (int)r;
-                if (b < a) continue;
-                const double *ca = src + (int64_t)a * n, *cb = src + (int64_t)b * n;
-                double s = 0.0;
-                for (int64_t k = 0; k < n; k++) s = fma(ca[k], cb[k], s);
-                G[a * r + b] = s;
-                G[b * r + a] = s;
+            // G = src^T src: four threads per (a, b) pair, strided over rows.
+            for (int task = t; task < 4 * ((npairs + 7) / 8) * 8; task += blockDim.x) {
+                const int pr = task >> 2, part = task & 3;
+                double sacc = 0.0;
+                int a = 0, b = 0;
+                if (pr < npairs) {
+                    // pr -> (a, b) with a <= b, row-major over the upper triangle.
+                    int rem = pr;
+                    a = 0;
+                    while (rem >= (int)r - a) {
+                        rem -= (int)r - a;
+                        a++;
+                    }
+                    b = a + rem;
+                    const double *ca = src + (int64_t)a * n, *cb = src + (int64_t)b * n;
+                    for (int64_t k = part; k < n; k += 4) sacc = fma(ca[k], cb[k], sacc);
+                }
+                sacc += __shfl_xor_sync(0xffffffffu, sacc, 1);
+                sacc += __shfl_xor_sync(0xffffffffu, sacc, 2);
+                if (pr < npairs && part == 0) {
+                    G[a * r + b] = sacc;
+                    G[b * r + a] = sacc;
+                }
             }
             __syncthreads();
             if (t < 32) {
-                const bool ok = warp_chol_inv(G, Ri, (int)r);
+                const bool ok = warp_chol_inv<RMAX>(G, Ri, (int)r);
                 if (t == 0) bad = ok ? 0 : 1;
             }
             __syncthreads();
@@ -221,27 +295,47 @@ __global__ void __launch_bounds__(LA_NT) subspace_kernel(const double *Sg, int64
             }
             for (int64_t e = t; e < n * r; e += blockDim.x) {
                 const int64_t i = e % n, c = e / n;
-                double s = 0.0;
-                for (int64_t k = 0; k <= c; k++) s = fma(src[i + k * n], Ri[k * r + c], s);
-                dst[e] = s;
+                double sacc = 0.0;
+                for (int64_t k = 0; k <= c; k++) sacc = fma(src[i + k * n], Ri[k * r + c], sacc);
+                dst[e] = sacc;
             }
             __syncthreads();
         }
         if (broke) {
-            // Householder on S L (still in Z when the first pass broke, in L
-            // when the second did): copy into the workspace and rebuild L.
-            const double *srcz = Z;
-            for (int64_t e = t; e < n * r; e += blockDim.x) hwork[e] = srcz[e];
+            // Householder on S L (Z holds it whichever pass broke).
+            for (int64_t e = t; e < n * r; e += blockDim.x) hwork[e] = Z[e];
             __syncthreads();
             hqr_device(hwork, n, r, hwork + n * r, L, red);
             if (t == 0 && flag) atomicOr(flag, 2);
             __syncthreads();
-        } else {
+        } else if (passes == 2) {
             for (int64_t e = t; e < n * r; e += blockDim.x) L[e] = Z[e];
             __syncthreads();
         }
     }
     for (int64_t e = t; e < n * r; e += blockDim.x) Lg[e] = L[e];
+}
+
+// Subspace iteration for ranks above 32: Householder QR every step, S, L and Z
+// in global memory (L2-resident).  work >= 3*n*r + r.
+__global__ void __launch_bounds__(LA_NT) subspace_wide_kernel(const double *S, int64_t n,
+                                                              double *L, int64_t r, int iters,
+                                                              double *work) {
+    __shared__ double red[33];
+    double *Z = work, *W = work + n * r, *tau = work + 2 * n * r;
+    for (int it = 0; it < iters; it++) {
+        for (int64_t e = threadIdx.x; e < n * r; e += blockDim.x) {
+            const int64_t i = e % n, c = e / n;
+            double acc = 0.0;
+            for (int64_t k = 0; k < n; k++) acc = fma(S[i + n * k], L[k + n * c], acc);
+            Z[e] = acc;
+        }
+        __syncthreads();
+        for (int64_t e = threadIdx.x; e < n * r; e += blockDim.x) W[e] = Z[e];
+        __syncthreads();
+        hqr_device(W, n, r, tau, L, red);
+        __syncthreads();
+    }
 }
 
 // LU with partial pivoting on W (n x n col-major copy of A), then Ainv by
@@ -339,7 +433,7 @@ __global__ void chol_lower_inv_kernel(const double *Gg, int r, double *Linv, int
     for (int e = threadIdx.x; e < r * r; e += blockDim.x) G[e] = Gg[e];  // symmetric
     __syncthreads();
     if (threadIdx.x < 32) {
-        const bool ok = warp_chol_inv(G, Ri, r);
+        const bool ok = warp_chol_inv<32>(G, Ri, r);
         if (!ok && threadIdx.x == 0) atomicOr(flag, 1);
     }
     __syncthreads();
@@ -347,6 +441,71 @@ __global__ void chol_lower_inv_kernel(const double *Gg, int r, double *Linv, int
     for (int e = threadIdx.x; e < r * r; e += blockDim.x) {
         const int i = e % r, c = e / r;  // Linv(i, c) = Rinv(c, i)
         Linv[e] = Ri[c * r + i];
+    }
+}
+
+// Row Gram of a tall factor stored transposed: A is r x m col-major, so
+// factor row k is the r contiguous values A[k*r ...].  Each block sums
+// u_k u_k^T over its rows into part[block][r*r]; entries are owned by threads.
+__global__ void __launch_bounds__(256) rows_gram_kernel(const double *__restrict__ A, int r,
+                                                        int64_t m, int64_t rows_per_block,
+                                                        double *__restrict__ part) {
+    __shared__ double us[64 * 33];
+    const int64_t k0 = blockIdx.x * rows_per_block;
+    const int64_t k1 = min(m, k0 + rows_per_block);
+    const int rr = r * r;
+    double acc[4] = {0, 0, 0, 0};  // entries t, t+256, t+512, t+768 (r <= 32)
+    for (int64_t kb = k0; kb < k1; kb += 64) {
+        const int nb = (int)(k1 - kb < 64 ? k1 - kb : 64);
+        __syncthreads();
+        for (int e = threadIdx.x; e < nb * r; e += blockDim.x) {
+            const int b = e / r, c = e - b * r;
+            us[b * 33 + c] = A[(kb + b) * r + c];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int e = threadIdx.x + 256 * q;
+            if (e >= rr) break;
+            const int a = e / r, c = e - a * r;
+            double sacc = acc[q];
+            for (int b = 0; b < nb; b++) sacc = fma(us[b * 33 + a], us[b * 33 + c], sacc);
+            acc[q] = sacc;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const int e = threadIdx.x + 256 * q;
+        if (e < rr) part[(int64_t)blockIdx.x * rr + e] = acc[q];
+    }
+}
+
+// T[:, k] = Linv A[:, k] for every factor row k (Linv lower, r x r col-major);
+// one thread per output element, out of place.
+__global__ void __launch_bounds__(256) rows_apply_kernel(const double *__restrict__ A, int r,
+                                                         int64_t m, const double *__restrict__ Linv,
+                                                         double *__restrict__ T) {
+    __shared__ double Ls[32 * 32];
+    for (int e = threadIdx.x; e < r * r; e += blockDim.x) Ls[e] = Linv[e];
+    __syncthreads();
+    const int64_t n = m * r;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = e / r;
+        const int a = (int)(e - k * r);
+        const double *u = A + k * r;
+        double acc = 0.0;
+        for (int c = 0; c <= a; c++) acc = fma(Ls[a + c * r], u[c], acc);
+        T[e] = acc;
+    }
+}
+
+__global__ void sum_parts_kernel(const double *__restrict__ part, int nblk, int n,
+                                 double *__restrict__ out) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+        double sacc = 0.0;
+        for (int b = 0; b < nblk; b++) sacc += part[(int64_t)b * n + e];
+        out[e] = sacc;
     }
 }
 
@@ -361,18 +520,39 @@ void householder_qr(dt_ctx *ctx, const double *A, int64_t m, int64_t n, double *
 
 void subspace_iter(dt_ctx *ctx, const double *S, int64_t n, double *L, int64_t r, int iters,
                    double *work, int *flag) {
-    DT_CHECK_ARG(n >= r && r > 0 && r <= 1024, "subspace_iter: bad sizes n=%lld r=%lld",
-                 (long long)n, (long long)r);
+    DT_CHECK_ARG(n >= r && r > 0, "subspace_iter: bad sizes n=%lld r=%lld", (long long)n,
+                 (long long)r);
+    if (r > 32) {
+        DT_LAUNCH(ctx, subspace_wide_kernel, 1, LA_NT, 0, S, n, L, r, iters, work);
+        return;
+    }
     const size_t base = 2 * r * r * sizeof(double);
-    const size_t s_bytes = n * n * sizeof(double);
+    const size_t full_bytes = n * n * sizeof(double);
+    const size_t packed_bytes = ((n * (n + 1) / 2 + 1) & ~int64_t(1)) * sizeof(double);
     const size_t zl_bytes = 2 * n * r * sizeof(double);
-    const size_t cap = 200 * 1024;
-    int s_in = base + s_bytes + zl_bytes <= cap;
-    int zl_in = base + (s_in ? s_bytes : 0) + zl_bytes <= cap;
-    const size_t smem = base + (s_in ? s_bytes : 0) + (zl_in ? zl_bytes : 0);
-    DT_CUDA(cudaFuncSetAttribute(subspace_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
-    DT_LAUNCH(ctx, subspace_kernel, 1, LA_NT, smem, S, n, L, r, iters, work, s_in, zl_in, flag);
+    const size_t cap = 220 * 1024;
+    int s_mode = S_GLOBAL;
+    size_t s_bytes = 0;
+    if (base + full_bytes + zl_bytes <= cap) {
+        s_mode = S_FULL;
+        s_bytes = full_bytes;
+    } else if (base + packed_bytes + zl_bytes <= cap) {
+        s_mode = S_PACKED;
+        s_bytes = packed_bytes;
+    }
+    const int zl_in = base + s_bytes + zl_bytes <= cap;
+    const size_t smem = base + s_bytes + (zl_in ? zl_bytes : 0);
+    if (r <= 16) {
+        DT_CUDA(cudaFuncSetAttribute(subspace_kernel<16>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        DT_LAUNCH(ctx, subspace_kernel<16>, 1, LA_NT, smem, S, n, L, r, iters, work, s_mode,
+                  zl_in, flag);
+    } else {
+        DT_CUDA(cudaFuncSetAttribute(subspace_kernel<32>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        DT_LAUNCH(ctx, subspace_kernel<32>, 1, LA_NT, smem, S, n, L, r, iters, work, s_mode,
+                  zl_in, flag);
+    }
 }
 
 void lu_inverse(dt_ctx *ctx, const double *A, int64_t n, double *Ainv, double *work,
@@ -388,9 +568,34 @@ void orth2_rows(dt_ctx *ctx, double *A, int64_t len1, int64_t len2) {
                  (long long)len1, (long long)len2);
     DevMem G(ctx, len1 * len1 * sizeof(double));
     DevMem Li(ctx, len1 * len1 * sizeof(double));
-    DevMem T(ctx, len1 * len2 * sizeof(double));
     DevMem flag(ctx, sizeof(int));
     DT_CUDA(cudaMemsetAsync(flag.get(), 0, sizeof(int), ctx->stream));
+    if (len1 <= 32) {
+        const int r = (int)len1;
+        const int64_t target = 2LL * ctx->num_sms;
+        const int64_t rpb = std::max<int64_t>(256, (len2 + target - 1) / target);
+        const int nblk = (int)((len2 + rpb - 1) / rpb);
+        DevMem part(ctx, (size_t)nblk * r * r * sizeof(double));
+        DevMem T(ctx, (size_t)r * len2 * sizeof(double));
+        const unsigned ablocks = std::max(
+            1u, std::min<unsigned>(ceil_div(len2 * r, 256), 16u * (unsigned)ctx->num_sms));
+        for (int pass = 0; pass < 2; pass++) {
+            const double *src = pass == 0 ? A : T.as<double>();
+            double *dst = pass == 0 ? T.as<double>() : A;
+            DT_LAUNCH(ctx, rows_gram_kernel, nblk, 256, 0, src, r, len2, rpb, part.as<double>());
+            DT_LAUNCH(ctx, sum_parts_kernel, 1, 256, 0, part.as<double>(), nblk, r * r,
+                      G.as<double>());
+            DT_LAUNCH(ctx, chol_lower_inv_kernel, 1, 256, 2 * r * r * sizeof(double),
+                      G.as<double>(), r, Li.as<double>(), flag.as<int>());
+            DT_LAUNCH(ctx, rows_apply_kernel, ablocks, 256, 0, src, r, len2, Li.as<double>(), dst);
+        }
+        int h = 0;
+        DT_CUDA(cudaMemcpyAsync(&h, flag.get(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        DT_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (h) fail(DT_ERR_NUMERIC, "orth2: rows are linearly dependent");
+        return;
+    }
+    DevMem T(ctx, len1 * len2 * sizeof(double));
     for (int pass = 0; pass < 2; pass++) {
         gemm_f64(ctx, 0, 1, len1, len1, len2, A, len1, A, len1, G.as<double>(), len1, 0.0);
         DT_LAUNCH(ctx, chol_lower_inv_kernel, 1, 256, 2 * len1 * len1 * sizeof(double),

@@ -1,0 +1,634 @@
+// Mixed-precision tensor-core kernels for the dense HOOI hot path (sm_100a):
+//
+//  * tc_ttm_kernel   Y = X x_n U^T with X in BF16 (hi, or hi+lo), U split into
+//                    BF16 hi+lo in shared memory, FP32 accumulation in TMEM.
+//                    The mode-n unfolding is never formed: TMA reads X either
+//                    K-major (mode 0, contracted index contiguous) or MN-major
+//                    (the rows of the output contiguous, 3-D box over
+//                    (l, i, b)), and the epilogue writes the result straight
+//                    into its destination layout (folded tensor, or the
+//                    K-major Y_(n) the Gram consumes).
+//  * tc_gram_kernel  split-K S = Y_(n) Y_(n)^T (+ the hi/lo cross term) with
+//                    both operands K-major; partial tiles reduced in FP64.
+//  * conversions     FP32 -> BF16 hi/lo (+ ||X||^2 in FP64), and the sweep core
+//                    G = U^T Y_(N-1) used for the convergence test.
+//
+// Warp roles in tc_ttm_kernel (192 threads): warp 0 issues TMA, warp 1 owns
+// TMEM and issues tcgen05.mma from one thread, warps 2-5 drain TMEM.  Every
+// mbarrier wait is bounded (dt_tc.cuh); on timeout the kernel records an error
+// and leaves after waiting (bounded) for the copies and MMAs it issued.
+#include <cuda.h>
+
+#include <algorithm>
+#include <cstring>
+
+#include "dt_tc.cuh"
+#include "dt_tc_host.cuh"
+
+namespace dt {
+namespace {
+
+using namespace tc;
+
+constexpr int TTM_THREADS = 192;
+constexpr int KC_ELEMS = 64;         // BF16 elements per 128-byte row
+constexpr int KC_BYTES = 128 * 128;  // one 128-row x 128-byte K-chunk of A
+
+__device__ __forceinline__ uint8_t *align1024(uint8_t *p) {
+    return reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(p) + 1023) & ~uintptr_t(1023));
+}
+
+__device__ __forceinline__ void bf16_split(float v, __nv_bfloat16 &hi, __nv_bfloat16 &lo) {
+    hi = __float2bfloat16_rn(v);
+    lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+}
+
+__device__ __forceinline__ int64_t out_rowbase(const OutMap &om, int64_t lp, int64_t bp) {
+    int64_t off = 0;
+    for (int d = 0; d < om.nl; d++) {
+        const int64_t q = lp / om.dl[d];
+        off += (lp - q * om.dl[d]) * om.sl[d];
+        lp = q;
+    }
+    for (int d = 0; d < om.nb; d++) {
+        const int64_t q = bp / om.db[d];
+        off += (bp - q * om.db[d]) * om.sb[d];
+        bp = q;
+    }
+    return off;
+}
+
+// ---------------------------------------------------------------------------
+// TTM
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(TTM_THREADS, 1)
+    tc_ttm_kernel(const __grid_constant__ CUtensorMap map_hi,
+                  const __grid_constant__ CUtensorMap map_lo, const TcTtmArgs a) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *sm = align1024(smem_raw);
+    const int S = a.stages;
+    uint8_t *Bt = sm;                                   // kchunks x Npad rows x 128 B
+    const uint32_t b_bytes = (uint32_t)a.kchunks * a.Npad * 128;
+    uint8_t *Abase = sm + ((b_bytes + 1023) & ~1023u);  // stages
+    const uint32_t a_one = (uint32_t)a.kchunks * KC_BYTES;
+    const uint32_t stage_bytes = a_one * (a.split ? 2 : 1);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(Abase + (size_t)S * stage_bytes);
+    uint64_t *full = bars, *empty = bars + S, *tfull = bars + 2 * S, *tempty = bars + 2 * S + 2;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * S + 4);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == 1) {
+        tmem_alloc(tmem_slot, a.tmem_cols);
+        tmem_relinquish();
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int i = 0; i < 2; i++) {
+            mbar_init(&tfull[i], 1);
+            mbar_init(&tempty[i], 128);
+        }
+        fence_mbar_init();
+    }
+    // B = [U_hi | U_lo]^T (split) or U_hi^T, K-major, 128B-swizzled, zero padded.
+    {
+        const int Jp = a.Jpad;
+        const int nrows = a.Npad;
+        const int kmax = a.kchunks * KC_ELEMS;
+        for (int e = threadIdx.x; e < nrows * kmax; e += blockDim.x) {
+            const int row = e / kmax, k = e - row * kmax;
+            const int j = row % Jp;
+            const bool lo_part = row >= Jp;
+            float v = 0.f;
+            if (j < a.J && k < a.I) v = (float)a.U[(int64_t)k + (int64_t)a.I * j];
+            __nv_bfloat16 hi, lo;
+            bf16_split(v, hi, lo);
+            const int kc = k / KC_ELEMS, kk = k - kc * KC_ELEMS;
+            uint8_t *dst = Bt + (uint32_t)kc * nrows * 128 + sw128_kmajor_offset(row, kk);
+            *reinterpret_cast<__nv_bfloat16 *>(dst) = lo_part ? lo : hi;
+        }
+    }
+    fence_proxy_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            prefetch_tmap(&map_hi);
+            if (a.split) prefetch_tmap(&map_lo);
+            int64_t k = 0;
+            bool ok = true;
+            for (int64_t tile = blockIdx.x; tile < a.ntiles && ok; tile += gridDim.x, k++) {
+                const int s = (int)(k % S);
+                if (k >= S) ok = mbar_wait(&empty[s], (uint32_t)(((k / S) - 1) & 1), a.err);
+                if (!ok) break;
+                mbar_expect_tx(&full[s], a.tx_bytes);
+                uint8_t *st = Abase + (size_t)s * stage_bytes;
+                if (a.kmajor) {
+                    const int r0 = (int)(tile * 128);
+                    for (int kc = 0; kc < a.kchunks; kc++) {
+                        tma_load_2d(st + kc * KC_BYTES, &map_hi, &full[s], kc * KC_ELEMS, r0);
+                        if (a.split)
+                            tma_load_2d(st + a_one + kc * KC_BYTES, &map_lo, &full[s],
+                                        kc * KC_ELEMS, r0);
+                    }
+                } else {
+                    const int64_t mb = tile % a.nmb, b = tile / a.nmb;
+                    const int l0 = (int)(mb * 128);
+                    for (int kc = 0; kc < a.kchunks; kc++)
+                        for (int h = 0; h < 2; h++) {
+                            uint8_t *d = st + kc * KC_BYTES + h * (KC_BYTES / 2);
+                            tma_load_3d(d, &map_hi, &full[s], l0 + h * 64, kc * KC_ELEMS, (int)b);
+                            if (a.split)
+                                tma_load_3d(d + a_one, &map_lo, &full[s], l0 + h * 64,
+                                            kc * KC_ELEMS, (int)b);
+                        }
+                }
+            }
+            // Leave no copy in flight: wait (bounded) for every stage issued.
+            const int64_t issued = k;
+            for (int64_t q = std::max<int64_t>(0, issued - S); q < issued; q++)
+                mbar_wait(&full[q % S], (uint32_t)((q / S) & 1), a.err);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t id_full = idesc_bf16(128, a.Npad, !a.kmajor, false);
+            const uint32_t id_half = idesc_bf16(128, a.Jpad, !a.kmajor, false);
+            int64_t k = 0;
+            bool ok = true;
+            for (int64_t tile = blockIdx.x; tile < a.ntiles && ok; tile += gridDim.x, k++) {
+                const int s = (int)(k % S);
+                const int acc = (int)(k & 1);
+                ok = mbar_wait(&full[s], (uint32_t)((k / S) & 1), a.err);
+                if (ok && k >= 2) ok = mbar_wait(&tempty[acc], (uint32_t)(((k / 2) - 1) & 1), a.err);
+                if (!ok) break;
+                tc_fence_after();
+                const uint32_t d = tmem_base + (uint32_t)(acc * a.Npad);
+                const uint32_t st = smem_u32(Abase + (size_t)s * stage_bytes);
+                const uint32_t bt = smem_u32(Bt);
+                for (int ks = 0; ks < a.ksteps; ks++) {
+                    const int kc = ks >> 2, sub = ks & 3;
+                    uint64_t ad, adl;
+                    if (a.kmajor) {
+                        ad = sdesc(st + kc * KC_BYTES + sub * 32, 16, 1024, kSwizzle128B);
+                        adl = sdesc(st + a_one + kc * KC_BYTES + sub * 32, 16, 1024, kSwizzle128B);
+                    } else {
+                        ad = sdesc(st + kc * KC_BYTES + sub * 2048, KC_BYTES / 2, 1024, kSwizzle128B);
+                        adl = sdesc(st + a_one + kc * KC_BYTES + sub * 2048, KC_BYTES / 2, 1024,
+                                    kSwizzle128B);
+                    }
+                    const uint64_t bd =
+                        sdesc(bt + (uint32_t)kc * a.Npad * 128 + sub * 32, 16, 1024, kSwizzle128B);
+                    umma_bf16(d, ad, bd, id_full, ks > 0 ? 1u : 0u);
+                    if (a.split) umma_bf16(d, adl, bd, id_half, 1u);
+                }
+                umma_commit(&empty[s]);
+                umma_commit(&tfull[acc]);
+            }
+            // Drain: the last two accumulators' MMAs must finish before dealloc.
+            const int64_t issued = k;
+            for (int64_t q = std::max<int64_t>(0, issued - 2); q < issued; q++)
+                mbar_wait(&tfull[q & 1], (uint32_t)((q / 2) & 1), a.err);
+        }
+    } else {
+        // Epilogue warps 2..5 -> TMEM lane quarters 2, 3, 0, 1.
+        const int quarter = warp & 3;
+        const int m = quarter * 32 + lane;
+        int64_t k = 0;
+        for (int64_t tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, k++) {
+            const int acc = (int)(k & 1);
+            if (!mbar_wait(&tfull[acc], (uint32_t)((k / 2) & 1), a.err)) break;
+            tc_fence_after();
+            const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * a.Npad);
+            float v[64];
+#pragma unroll
+            for (int g = 0; g < 4; g++) {
+                if (g * 16 < a.Npad) {
+                    float tmp[16];
+                    tmem_ld16(taddr + g * 16, tmp);
+#pragma unroll
+                    for (int i = 0; i < 16; i++) v[g * 16 + i] = tmp[i];
+                }
+            }
+            tmem_wait_ld();
+            tc_fence_before();
+            mbar_arrive(&tempty[acc]);
+            if (a.split) {
+#pragma unroll
+                for (int j = 0; j < 32; j++)
+                    if (j < a.Jpad) v[j] += v[a.Jpad + j];
+            }
+            int64_t lp, bp;
+            bool valid;
+            if (a.kmajor) {
+                lp = 0;
+                bp = tile * 128 + m;
+                valid = bp < a.B;
+            } else {
+                const int64_t mb = tile % a.nmb;
+                lp = mb * 128 + m;
+                bp = tile / a.nmb;
+                valid = lp < a.L;
+            }
+            if (!valid) continue;
+            const int64_t base = out_rowbase(a.om, lp, bp);
+            if (a.out_f32) {
+#pragma unroll
+                for (int j = 0; j < 32; j++)
+                    if (j < a.J) a.out_f32[base + j * a.om.jstride] = v[j];
+            } else {
+#pragma unroll
+                for (int j = 0; j < 32; j++) {
+                    if (j < a.J) {
+                        __nv_bfloat16 hi, lo;
+                        bf16_split(v[j], hi, lo);
+                        a.out_hi[base + j * a.om.jstride] = hi;
+                        if (a.out_lo) a.out_lo[base + j * a.om.jstride] = lo;
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem_base, a.tmem_cols);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Gram: part[z] = Yh Yh^T (and Yh Yl^T in the second half of the columns),
+// over this CTA's K-range.  A = rows [0, 128) of the staged Y tile, B = the
+// first N rows (Yh rows, then Yl rows, placed back to back).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128, 1)
+    tc_gram_kernel(const __grid_constant__ CUtensorMap map_hi,
+                   const __grid_constant__ CUtensorMap map_lo, const TcGramArgs a) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *sm = align1024(smem_raw);
+    const int nck = a.chunks_per_cta;
+    const int64_t c0 = (int64_t)blockIdx.x * nck;
+    const int64_t c1 = std::min<int64_t>(a.kchunks_total, c0 + nck);
+    const int n_my = (int)std::max<int64_t>(0, c1 - c0);
+    const uint32_t rows_bytes = (uint32_t)a.Ipad * 128;
+    const uint32_t chunk_bytes = a.chunk_bytes;  // >= 128 rows and >= (split ? 2 : 1) * Ipad rows
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sm + (size_t)nck * chunk_bytes);
+    uint64_t *full = bars, *done = bars + nck;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + nck + 1);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == 0) {
+        tmem_alloc(tmem_slot, a.tmem_cols);
+        tmem_relinquish();
+    }
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < nck; c++) mbar_init(&full[c], 1);
+        mbar_init(done, 1);
+        fence_mbar_init();
+    }
+    // Zero the chunk buffers: A reads 128 rows, of which only the first Ipad
+    // (or 2*Ipad) are loaded.
+    for (uint32_t e = threadIdx.x; e < (uint32_t)nck * chunk_bytes / 16; e += blockDim.x)
+        reinterpret_cast<uint4 *>(sm)[e] = make_uint4(0, 0, 0, 0);
+    fence_proxy_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    bool ok = true;
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < n_my; c++) {
+            mbar_expect_tx(&full[c], a.tx_bytes);
+            uint8_t *dst = sm + (size_t)c * chunk_bytes;
+            tma_load_2d(dst, &map_hi, &full[c], (int)((c0 + c) * KC_ELEMS), 0);
+            if (a.split) tma_load_2d(dst + rows_bytes, &map_lo, &full[c], (int)((c0 + c) * KC_ELEMS), 0);
+        }
+        const uint32_t idesc = idesc_bf16(128, a.N, false, false);
+        for (int c = 0; c < n_my && ok; c++) {
+            ok = mbar_wait(&full[c], 0, a.err);
+            if (!ok) break;
+            tc_fence_after();
+            const uint32_t base = smem_u32(sm + (size_t)c * chunk_bytes);
+            for (int sub = 0; sub < 4; sub++) {
+                const uint64_t ad = sdesc(base + sub * 32, 16, 1024, kSwizzle128B);
+                umma_bf16(tmem_base, ad, ad, idesc, (c > 0 || sub > 0) ? 1u : 0u);
+            }
+        }
+        if (ok && n_my > 0) umma_commit(done);
+        if (!ok) {
+            for (int c = 0; c < n_my; c++) mbar_wait(&full[c], 0, a.err);
+        }
+    }
+    __syncthreads();
+    if (n_my > 0 && mbar_wait(done, 0, a.err)) {
+        tc_fence_after();
+        const int m = warp * 32 + lane;
+        float *dst = a.part + (int64_t)blockIdx.x * a.Ipad * a.N + (int64_t)m * a.N;
+        for (int g = 0; g < a.N; g += 16) {
+            float v[16];
+            tmem_ld16(tmem_base + ((uint32_t)(warp * 32) << 16) + g, v);
+            tmem_wait_ld();
+            if (m < a.Ipad) {
+#pragma unroll
+                for (int i = 0; i < 16; i++) dst[g + i] = v[i];
+            }
+        }
+    } else if (n_my == 0) {
+        const int m = warp * 32 + lane;
+        if (m < a.Ipad)
+            for (int g = 0; g < a.N; g++)
+                a.part[(int64_t)blockIdx.x * a.Ipad * a.N + (int64_t)m * a.N + g] = 0.f;
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        tmem_dealloc(tmem_base, a.tmem_cols);
+    }
+}
+
+// S[i + n*j] = sum_z part[z][i][j] (+ part[z][i][Ipad+j] + part[z][j][Ipad+i]).
+__global__ void gram_reduce_kernel(const float *__restrict__ part, int nz, int n, int Ipad, int N,
+                                   int split, double *__restrict__ S) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n * n; e += gridDim.x * blockDim.x) {
+        const int i = e % n, j = e / n;
+        double s = 0.0;
+        for (int z = 0; z < nz; z++) {
+            const float *p = part + (int64_t)z * Ipad * N;
+            s += (double)p[i * N + j];
+            if (split) s += (double)p[i * N + Ipad + j] + (double)p[j * N + Ipad + i];
+        }
+        S[e] = s;
+    }
+}
+
+// X (FP32) -> BF16 hi (+ lo) and per-block partial sums of squares (FP64).
+__global__ void split_f32_kernel(const float *__restrict__ x, int64_t n,
+                                 __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo,
+                                 double *__restrict__ part) {
+    double s = 0.0;
+    const int64_t n4 = n / 4;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n4;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const float4 v = reinterpret_cast<const float4 *>(x)[e];
+        __nv_bfloat16 h[4], l[4];
+        bf16_split(v.x, h[0], l[0]);
+        bf16_split(v.y, h[1], l[1]);
+        bf16_split(v.z, h[2], l[2]);
+        bf16_split(v.w, h[3], l[3]);
+        reinterpret_cast<uint2 *>(hi)[e] = *reinterpret_cast<uint2 *>(h);
+        if (lo) reinterpret_cast<uint2 *>(lo)[e] = *reinterpret_cast<uint2 *>(l);
+        s = fma((double)v.x, (double)v.x, s);
+        s = fma((double)v.y, (double)v.y, s);
+        s = fma((double)v.z, (double)v.z, s);
+        s = fma((double)v.w, (double)v.w, s);
+    }
+    for (int64_t e = n4 * 4 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const float v = x[e];
+        __nv_bfloat16 h, l;
+        bf16_split(v, h, l);
+        hi[e] = h;
+        if (lo) lo[e] = l;
+        s = fma((double)v, (double)v, s);
+    }
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) part[blockIdx.x] = s;
+    }
+}
+
+// Sweep core from the K-major leaf rows: G[k + K*r] = sum_i Y[i][k] U[i][r]
+// (FP32 accumulate), one thread per (k, r); per-block partial sum of G^2 in
+// FP64.
+__global__ void __launch_bounds__(256) core_rows_kernel(const __nv_bfloat16 *__restrict__ Yh,
+                                                        const __nv_bfloat16 *__restrict__ Yl,
+                                                        int64_t I, int64_t K,
+                                                        const double *__restrict__ U, int R,
+                                                        double *__restrict__ G,
+                                                        double *__restrict__ part) {
+    extern __shared__ float Us[];  // I x R
+    for (int64_t e = threadIdx.x; e < I * R; e += blockDim.x) Us[e] = (float)U[e];
+    __syncthreads();
+    double s2 = 0.0;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < K * R;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = e % K;
+        const int r = (int)(e / K);
+        const float *u = Us + (int64_t)I * r;
+        float acc = 0.f;
+        for (int64_t i = 0; i < I; i++) {
+            float y = __bfloat162float(Yh[i * K + k]);
+            if (Yl) y += __bfloat162float(Yl[i * K + k]);
+            acc = fmaf(y, u[i], acc);
+        }
+        G[k + K * r] = acc;
+        s2 = fma((double)acc, (double)acc, s2);
+    }
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) s2 += __shfl_down_sync(0xffffffffu, s2, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s2;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s2 = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) s2 += __shfl_down_sync(0xffffffffu, s2, o);
+        if (threadIdx.x == 0) part[blockIdx.x] = s2;
+    }
+}
+
+__global__ void sum_double_kernel(const double *__restrict__ part, int n, double *__restrict__ out) {
+    double s = 0.0;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) s += part[e];
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) out[0] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side: tensor maps and launchers.
+// ---------------------------------------------------------------------------
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        DT_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        if (!p || q != cudaDriverEntryPointSuccess)
+            fail(DT_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+        fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+CUtensorMap make_map(const void *base, int rank, const uint64_t *dims, const uint64_t *strides_bytes,
+                     const uint32_t *box) {
+    CUtensorMap m;
+    std::memset(&m, 0, sizeof(m));
+    cuuint64_t gd[5], gs[4];
+    cuuint32_t bx[5], es[5];
+    for (int i = 0; i < rank; i++) {
+        gd[i] = dims[i];
+        bx[i] = box[i];
+        es[i] = 1;
+    }
+    for (int i = 0; i < rank - 1; i++) gs[i] = strides_bytes[i];
+    const CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, (cuuint32_t)rank,
+                                   const_cast<void *>(base), gd, gs, bx, es,
+                                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) fail(DT_ERR_CUDA, fmt("cuTensorMapEncodeTiled failed (%d)", (int)r));
+    return m;
+}
+
+int pad16(int v) { return (v + 15) & ~15; }
+
+}  // namespace
+
+bool tc_ttm_supported(int64_t L, int64_t I, int64_t B, int64_t J) {
+    if (J < 1 || J > 32 || I < 1) return false;
+    if (I > 64 * 64) return false;  // keeps one stage of A within shared memory
+    if (L == 1) return (I % 8) == 0 && B >= 1 && B < (int64_t(1) << 31);
+    return L >= 64 && (L % 8) == 0 && L < (int64_t(1) << 31) && B < (int64_t(1) << 31) &&
+           I < (int64_t(1) << 31);
+}
+
+void tc_ttm(dt_ctx *ctx, const __nv_bfloat16 *Xh, const __nv_bfloat16 *Xl, int64_t L, int64_t I,
+            int64_t B, const double *U, int64_t J, const OutMap &om, __nv_bfloat16 *out_hi,
+            __nv_bfloat16 *out_lo, float *out_f32, int *err) {
+    DT_CHECK_ARG(tc_ttm_supported(L, I, B, J), "tc_ttm: unsupported shape L=%lld I=%lld J=%lld",
+                 (long long)L, (long long)I, (long long)J);
+    TcTtmArgs a{};
+    a.kmajor = L == 1;
+    a.L = L;
+    a.I = I;
+    a.B = B;
+    a.J = (int)J;
+    a.Jpad = pad16((int)J);
+    a.split = Xl != nullptr;
+    a.Npad = a.split ? 2 * a.Jpad : a.Jpad;
+    a.kchunks = (int)((I + KC_ELEMS - 1) / KC_ELEMS);
+    a.ksteps = (int)((I + 15) / 16);
+    a.nmb = a.kmajor ? (B + 127) / 128 : (L + 127) / 128;
+    a.ntiles = a.kmajor ? a.nmb : a.nmb * B;
+    a.U = U;
+    a.out_hi = out_hi;
+    a.out_lo = out_lo;
+    a.out_f32 = out_f32;
+    a.om = om;
+    a.err = err;
+    int cols = 32;
+    while (cols < 2 * a.Npad) cols *= 2;
+    a.tmem_cols = cols;
+    const uint32_t a_one = (uint32_t)a.kchunks * KC_BYTES;
+    const uint32_t stage_bytes = a_one * (a.split ? 2 : 1);
+    const uint32_t b_bytes = ((uint32_t)a.kchunks * a.Npad * 128 + 1023) & ~1023u;
+    const size_t budget = 220 * 1024;
+    int S = (int)std::min<size_t>(4, (budget - b_bytes - 1024 - 256) / stage_bytes);
+    DT_CHECK_ARG(S >= 2, "tc_ttm: contraction length %lld too large for shared memory", (long long)I);
+    a.stages = S;
+    // Bytes the TMA delivers per stage (boxes are counted whole, OOB included).
+    a.tx_bytes = stage_bytes;
+    CUtensorMap mh, ml;
+    if (a.kmajor) {
+        const uint64_t dims[2] = {(uint64_t)I, (uint64_t)B};
+        const uint64_t str[1] = {(uint64_t)I * 2};
+        const uint32_t box[2] = {KC_ELEMS, 128};
+        mh = make_map(Xh, 2, dims, str, box);
+        ml = Xl ? make_map(Xl, 2, dims, str, box) : mh;
+    } else {
+        const uint64_t dims[3] = {(uint64_t)L, (uint64_t)I, (uint64_t)B};
+        const uint64_t str[2] = {(uint64_t)L * 2, (uint64_t)L * I * 2};
+        const uint32_t box[3] = {64, KC_ELEMS, 1};
+        mh = make_map(Xh, 3, dims, str, box);
+        ml = Xl ? make_map(Xl, 3, dims, str, box) : mh;
+    }
+    const size_t smem = 1024 + b_bytes + (size_t)S * stage_bytes + (2 * S + 4) * 8 + 16;
+    DT_CUDA(cudaFuncSetAttribute(tc_ttm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+    const unsigned grid = (unsigned)std::min<int64_t>(a.ntiles, ctx->num_sms);
+    DT_LAUNCH(ctx, tc_ttm_kernel, grid, TTM_THREADS, smem, mh, ml, a);
+}
+
+bool tc_gram_supported(int64_t I, int64_t K) {
+    return I >= 1 && I <= 128 && (K % 8) == 0 && K >= 1 && K < (int64_t(1) << 31);
+}
+
+void tc_gram(dt_ctx *ctx, const __nv_bfloat16 *Yh, const __nv_bfloat16 *Yl, int64_t I, int64_t K,
+             double *S, int *err) {
+    DT_CHECK_ARG(tc_gram_supported(I, K), "tc_gram: unsupported I=%lld K=%lld", (long long)I,
+                 (long long)K);
+    TcGramArgs a{};
+    a.split = Yl != nullptr;
+    a.Ipad = (int)((I + 7) & ~int64_t(7));
+    a.N = pad16(a.split ? 2 * a.Ipad : a.Ipad);
+    a.kchunks_total = (K + KC_ELEMS - 1) / KC_ELEMS;
+    // At most 16 partial tiles: the MMA work is small, the FP64 reduction of
+    // the partials is what grows with the split.
+    const int64_t target = 16;
+    int nck = (int)std::max<int64_t>(1, (a.kchunks_total + target - 1) / target);
+    a.chunk_bytes = (uint32_t)std::max<int64_t>(KC_BYTES, (a.split ? 2 : 1) * a.Ipad * 128);
+    a.chunk_bytes = (a.chunk_bytes + 1023) & ~1023u;
+    while (nck > 1 && (size_t)nck * a.chunk_bytes > 200 * 1024) nck--;
+    const int64_t nz = (a.kchunks_total + nck - 1) / nck;
+    a.chunks_per_cta = nck;
+    a.tx_bytes = (uint32_t)((a.split ? 2 : 1) * a.Ipad * 128);
+    int cols = 32;
+    while (cols < a.N) cols *= 2;
+    a.tmem_cols = cols;
+    a.err = err;
+    DevMem part(ctx, (size_t)nz * a.Ipad * a.N * sizeof(float));
+    a.part = part.as<float>();
+    const uint64_t dims[2] = {(uint64_t)K, (uint64_t)I};
+    const uint64_t str[1] = {(uint64_t)K * 2};
+    const uint32_t box[2] = {KC_ELEMS, (uint32_t)a.Ipad};
+    CUtensorMap mh = make_map(Yh, 2, dims, str, box);
+    CUtensorMap ml = Yl ? make_map(Yl, 2, dims, str, box) : mh;
+    const size_t smem = 1024 + (size_t)nck * a.chunk_bytes + (nck + 2) * 8 + 16;
+    DT_CUDA(cudaFuncSetAttribute(tc_gram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+    DT_LAUNCH(ctx, tc_gram_kernel, (unsigned)nz, 128, smem, mh, ml, a);
+    const int n = (int)I;
+    DT_LAUNCH(ctx, gram_reduce_kernel, std::max(1u, ceil_div((int64_t)n * n, 256)), 256, 0,
+              a.part, (int)nz, n, a.Ipad, a.N, a.split, S);
+}
+
+void split_f32(dt_ctx *ctx, const float *x, int64_t n, __nv_bfloat16 *hi, __nv_bfloat16 *lo,
+               double *sumsq_out) {
+    const int blocks = std::max(1, std::min<int>(4 * ctx->num_sms, (int)ceil_div(n / 4 + 1, 256)));
+    DevMem part(ctx, (size_t)blocks * sizeof(double));
+    DT_LAUNCH(ctx, split_f32_kernel, blocks, 256, 0, x, n, hi, lo, part.as<double>());
+    DT_LAUNCH(ctx, sum_double_kernel, 1, 1024, 0, part.as<double>(), blocks, sumsq_out);
+}
+
+void core_rows(dt_ctx *ctx, const __nv_bfloat16 *Yh, const __nv_bfloat16 *Yl, int64_t I, int64_t K,
+               const double *U, int64_t R, double *G, double *g2_out) {
+    DT_CHECK_ARG(R <= 32, "core_rows: R %lld > 32", (long long)R);
+    const int blocks = std::max(1, std::min<int>(4 * ctx->num_sms, (int)ceil_div(K * R, 256)));
+    DevMem part(ctx, (size_t)blocks * sizeof(double));
+    DT_LAUNCH(ctx, core_rows_kernel, blocks, 256, I * R * sizeof(float), Yh, Yl, I, K, U, (int)R,
+              G, part.as<double>());
+    DT_LAUNCH(ctx, sum_double_kernel, 1, 1024, 0, part.as<double>(), blocks, g2_out);
+}
+
+}  // namespace dt

@@ -70,6 +70,8 @@ typedef struct {
     int refine_sweeps;  /* BF16 modes: the last sweeps (after the tol test first
                            passes) run with hi+lo operands; 0 = none */
     int verbose;        /* print one line per sweep to stderr */
+    int profile;        /* record CUDA events around every TTM launch that
+                           streams X (reported as ttm_x_*) */
 } dt_hooi_opts;
 
 #define DT_MAX_HIST 256
@@ -81,6 +83,13 @@ typedef struct {
     double device_ms;             /* CUDA-event time of the whole decomposition */
     double res_hist[DT_MAX_HIST]; /* per-sweep residual as tracked by the sweep */
     int kernel_launches;          /* kernels launched by the decomposition */
+    int precision_used;           /* DT_PREC_* actually run (a tensor-core request
+                                     falls back to FP64 for shapes outside the
+                                     TMA / UMMA layout rules) */
+    int ttm_x_launches;           /* with opts.profile: TTM launches that read X */
+    double ttm_x_ms;              /* ... their summed CUDA-event time */
+    double ttm_x_bytes;           /* ... their summed algorithmic bytes
+                                     (X read + output written + factor read) */
 } dt_hooi_report;
 
 /* ---- context ---------------------------------------------------------- */
@@ -145,6 +154,23 @@ DT_API int dt_orth2_f64(dt_ctx *ctx, double *A, int64_t len1, int64_t len2);
  * subspace. */
 DT_API int dt_als_f64(dt_ctx *ctx, const double *Y, int ndim, const int64_t *shape, int mode,
                const double *L0, int64_t R, int iters, double *Q);
+
+/* ---- tensor-core (sm_100a tcgen05) operators ---------------------------- */
+/* Y = X x_mode U^T on the tensor cores: X (FP32, column-major) is rounded to
+ * BF16 (split = 0) or split into BF16 hi + lo (split = 1), U (shape[mode] x J
+ * col-major, FP64) likewise; FP32 accumulation; Y (FP32) folded like X with
+ * shape[mode] -> J.  The mixed-precision form of Function::ttm
+ * (tensor.tpp:272-335) used by the BF16 HOOI.  DT_ERR_UNSUPPORTED when the
+ * layout falls outside the TMA rules (mode 0 needs shape[0] % 8 == 0; other
+ * modes need prod_{m<mode} shape[m] >= 64 and % 8 == 0; J <= 32). */
+DT_API int dt_ttm_tc(dt_ctx *ctx, const float *X, int ndim, const int64_t *shape, int mode,
+                     const double *U, int64_t J, int split, float *Y);
+
+/* S (I x I, FP64) = Y Y^T for a row-major I x K FP32 Y, on the tensor cores
+ * (BF16 or split hi+lo operands, FP32 accumulation, FP64 reduction of the
+ * split-K partials).  The Gram of Function::gram (tensor.tpp:18-120) for
+ * I <= 128, K % 8 == 0. */
+DT_API int dt_gram_tc(dt_ctx *ctx, const float *Y, int64_t I, int64_t K, int split, double *S);
 
 /* ---- dense HOOI ------------------------------------------------------- */
 /* Tucker decomposition of X (dtype DT_F64 or DT_F32, column-major) with the
