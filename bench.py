@@ -4,9 +4,9 @@
 Workload: the 96x96x96x96 FP32 Tucker tensor (core 16^4 N(0,1) scaled by
 0.9^(i+j+k+l), QR'd Gaussian factors, noise N(0,1e-6), seed 1), HOOI ranks
 16^4.  A step is one whole decomposition with X resident in HBM: BF16 hi/lo
-split of X, libc-seeded random orthonormal init, BF16 tensor-core sweeps until
-the residual settles, split-BF16 refinement sweeps, FP64 subspace iteration
-per mode, and the final FP64 core projection -- until the relative
+split of X, libc-seeded random orthonormal init, split-BF16 tensor-core
+sweeps (TTM chain and Gram) until the residual settles, FP64 subspace
+iteration per mode, and the final FP64 core projection -- until the relative
 reconstruction error is within 1e-6 of the FP64 oracle's (checked every run).
 
 One JSON line on rank 0:
@@ -42,6 +42,10 @@ RANKS = (16, 16, 16, 16)
 SHAPE = (96, 96, 96, 96)
 TARGET = 1e-6
 FALLBACK_HBM_GBS = 6650.0
+
+
+def _log(msg):
+    print(f"[bench {time.strftime('%H:%M:%S')}] {msg}", file=sys.stderr, flush=True)
 
 
 def _peaks():
@@ -154,7 +158,7 @@ def run_ours(args):
     import numpy as np
     import torch
 
-    from diana_tucker_b200 import DT_PREC_BF16, DT_PREC_FP64, Context, datasets
+    from diana_tucker_b200 import DT_PREC_BF16X2, DT_PREC_FP64, Context, datasets
 
     world, rank, local = _dist_setup(args.gpus)
     torch.cuda.set_device(local)
@@ -164,16 +168,19 @@ def run_ours(args):
     Xd = torch.from_numpy(flat).to(f"cuda:{local}")
     kw = dict(init="randn", seed=1, max_sweeps=30, tol=1e-9, inner_iters=5, shape=SHAPE)
 
-    def mixed(profile=False):
-        return ctx.hooi_dense(Xd, RANKS, precision=DT_PREC_BF16, refine_sweeps=2,
-                              profile=profile, **kw)
+    X64d = Xd.double()  # the FP64 drop-in takes Tensor<double>
 
-    def fp64(profile=False):
-        return ctx.hooi_dense(Xd, RANKS, precision=DT_PREC_FP64, profile=profile, **kw)
+    def mixed(profile=False):
+        return ctx.hooi_dense(Xd, RANKS, precision=DT_PREC_BF16X2, profile=profile, **kw)
+
+    def fp64(profile=False, x=X64d):
+        return ctx.hooi_dense(x, RANKS, precision=DT_PREC_FP64, profile=profile, **kw)
 
     # Warm-up (module loading, memory pool).
+    _log("warm-up")
     for _ in range(args.warmup):
         mixed()
+    _log("timed region")
     # Timed region: K whole decompositions, device time by CUDA events on the
     # stream the library runs on, max over ranks.
     clocks = ClockSampler(local)
@@ -196,20 +203,31 @@ def run_ours(args):
     ms = _max_over_ranks(ms, world, local)
     rep = reps[-1]
 
-    # FP64 GPU path, same tensor and stopping rule.
+    _log(f"mixed {ms:.3f} ms/decomposition; FP64 path")
+    # FP64 GPU path, same tensor and stopping rule: X stored in FP64 (the
+    # drop-in's Tensor<double>) and, for reference, FP64 arithmetic reading
+    # the FP32-stored X.
     fp64()
     t64 = []
     for _ in range(max(1, min(args.steps, 3))):
-        _, _, r64 = fp64(profile=True)
+        _, _, r64 = fp64()
         t64.append(r64["device_ms"])
     fp64_ms = float(np.median(t64))
+    fp64(x=Xd)
+    t32 = []
+    for _ in range(max(1, min(args.steps, 3))):
+        _, _, r32 = fp64(x=Xd)
+        t32.append(r32["device_ms"])
+    fp64_x32_ms = float(np.median(t32))
+    del X64d
 
+    _log("end to end from pinned host memory")
     # End to end through the public API from pinned host memory.
     Xh = torch.from_numpy(flat).pin_memory()
     e2e_t = []
     for i in range(max(1, min(args.steps, 3)) + 1):
         t0 = time.perf_counter()
-        G, U, _ = ctx.hooi_dense(Xh, RANKS, precision=DT_PREC_BF16, refine_sweeps=2, **kw)
+        G, U, _ = ctx.hooi_dense(Xh, RANKS, precision=DT_PREC_BF16X2, **kw)
         dt = (time.perf_counter() - t0) * 1e3
         if i > 0:
             e2e_t.append(dt)
@@ -250,7 +268,8 @@ def run_ours(args):
                         "seed 1; HOOI ranks 16^4; BF16 tcgen05 TTM chain + Gram with split "
                         "hi/lo refinement, FP64 subspace iteration / fit / final core",
             "init": "libc-seeded Gaussian + QR (seed 1)",
-            "stop": "BF16 sweeps until the residual settles to 1e-3, then 2 split sweeps",
+            "stop": "split hi+lo BF16 sweeps until the residual changes by < 5e-6 "
+                    "(the split-precision noise floor); then the FP64 core projection",
             "target": f"|rel-err - FP64 oracle rel-err| <= {TARGET}",
             "l2": "inputs larger than L2 (X: 340 MB FP32, 170 MB per BF16 half; L2 126 MB)",
             "parallelism": f"replicas x{world} (no data-path collective)",
@@ -261,7 +280,10 @@ def run_ours(args):
         "target_met": bool(err <= TARGET),
         "sweeps": rep["sweeps"],
         "fp64_gpu": {"ms": round(fp64_ms, 4), "rel_err": r64["residual"], "sweeps": r64["sweeps"],
-                     "speedup_mixed_vs_fp64": round(fp64_ms / ms, 3) if ms > 0 else None},
+                     "x_dtype": "f64",
+                     "speedup_mixed_vs_fp64": round(fp64_ms / ms, 3) if ms > 0 else None,
+                     "ms_x_f32": round(fp64_x32_ms, 4),
+                     "speedup_mixed_vs_fp64_x_f32": round(fp64_x32_ms / ms, 3) if ms > 0 else None},
         "decompositions_per_s": round(world * 1000.0 / ms, 3) if ms > 0 else None,
         "e2e": {"value": round(e2e_ms, 4), "unit": "ms", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
@@ -278,9 +300,12 @@ def run_ours(args):
     if clk:
         out["clocks"] = clk
     if args.ttmc and world == 1:
+        _log("sparse TTMc")
         out["ttmc"] = _ttmc(ctx, peak)
     if rank == 0 and world == 1 and args.cpu:
+        _log("CPU baseline (reference HOOI_ALS, one sweep)")
         out["cpu_baseline"] = _cpu_baseline(X, oracle_sweeps or r64["sweeps"])
+    _log("done")
     ctx.close()
     if world > 1:
         import torch.distributed as dist

@@ -282,6 +282,51 @@ class Context:
                                           Uptr, ctypes.byref(rep)))
         return G, U, rep.as_dict()
 
+    # -- batched ---------------------------------------------------------------
+    def hooi_batched(self, tensors, ranks, U0, sweeps=10, inner_iters=5, block_threads=0):
+        """HOOI of many small 3-way tensors in one launch (dt_hooi_batched).
+        tensors: list of FP32 arrays; ranks: list of 3-tuples; U0: list of
+        3-lists of initial factors.  Returns (U, G, relerr, report)."""
+        count = len(tensors)
+        shapes = np.array([t.shape for t in tensors], dtype=np.int64).reshape(-1)
+        rk = np.array(ranks, dtype=np.int64).reshape(-1)
+        xs = [np.asfortranarray(t, dtype=np.float32).reshape(-1, order="F") for t in tensors]
+        xoff = np.zeros(count, dtype=np.int64)
+        xoff[1:] = np.cumsum([x.size for x in xs])[:-1]
+        X = np.concatenate(xs)
+        ublocks, uoff = [], []
+        o = 0
+        for t in range(count):
+            for n in range(3):
+                u = np.asfortranarray(U0[t][n], dtype=np.float64).reshape(-1, order="F")
+                ublocks.append(u)
+                uoff.append(o)
+                o += u.size
+        U = np.concatenate(ublocks)
+        uoff = np.array(uoff, dtype=np.int64)
+        gsz = [int(np.prod(r)) for r in ranks]
+        goff = np.zeros(count, dtype=np.int64)
+        goff[1:] = np.cumsum(gsz)[:-1]
+        G = np.zeros(int(sum(gsz)))
+        relerr = np.zeros(count)
+        rep = _lib.BatchedReport()
+        _lib.check(self.lib.dt_hooi_batched(
+            self.h, count, _i64p(shapes), _i64p(rk), X.ctypes.data, _i64p(xoff), sweeps,
+            inner_iters, U.ctypes.data, _i64p(uoff), G.ctypes.data, _i64p(goff),
+            relerr.ctypes.data, block_threads, ctypes.byref(rep)))
+        Uo, Go = [], []
+        for t in range(count):
+            fac = []
+            for n in range(3):
+                I, R = tensors[t].shape[n], ranks[t][n]
+                fac.append(np.reshape(U[uoff[3 * t + n]:uoff[3 * t + n] + I * R], (I, R), order="F"))
+            Uo.append(fac)
+            Go.append(np.reshape(G[goff[t]:goff[t] + gsz[t]], ranks[t], order="F"))
+        report = {"device_ms": rep.device_ms, "block_threads": rep.block_threads,
+                  "grid": rep.grid, "kernel_launches": rep.kernel_launches,
+                  "tune_ms": list(rep.tune_ms)}
+        return Uo, Go, relerr, report
+
     # -- sparse ----------------------------------------------------------------
     def sptensor(self, idx, vals, shape):
         return SpTensor(self, idx, vals, shape)

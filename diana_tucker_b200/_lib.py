@@ -81,6 +81,16 @@ class HooiReport(ctypes.Structure):
         }
 
 
+class BatchedReport(ctypes.Structure):
+    _fields_ = [
+        ("device_ms", ctypes.c_double),
+        ("block_threads", ctypes.c_int),
+        ("grid", ctypes.c_int),
+        ("kernel_launches", ctypes.c_int),
+        ("tune_ms", ctypes.c_double * 3),
+    ]
+
+
 # (name, restype, argtypes)
 _vp = ctypes.c_void_p
 _SIGS = [
@@ -110,6 +120,9 @@ _SIGS = [
                                      ctypes.POINTER(HooiOpts), _vp, ctypes.POINTER(_vp),
                                      ctypes.POINTER(HooiReport)]),
     ("dt_hooi_default_opts", None, [ctypes.POINTER(HooiOpts)]),
+    ("dt_hooi_batched", ctypes.c_int, [_vp, ctypes.c_int, c_i64p, c_i64p, _vp, c_i64p,
+                                       ctypes.c_int, ctypes.c_int, _vp, c_i64p, _vp, c_i64p,
+                                       _vp, ctypes.c_int, ctypes.POINTER(BatchedReport)]),
     ("dt_sptensor_create", ctypes.c_int, [_vp, ctypes.c_int64, ctypes.c_int,
                                           ctypes.POINTER(_vp), _vp, c_i64p,
                                           ctypes.POINTER(_vp)]),

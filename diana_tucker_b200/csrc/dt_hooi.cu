@@ -188,19 +188,25 @@ void DenseHooi::init_factors(double *const *U_user) {
     }
     if (opts.init == DT_INIT_RANDN_LIBC) {
         // hooi_als.tpp:74-81: U_rand(I_n x R_n).randn(); U_n = Q of reduced_QR.
-        srand(opts.seed);
-        DevMem tmp(ctx, 0);
+        if (opts.seed != DT_SEED_KEEP) srand(opts.seed);
+        // Draw every block in mode order (the reference's order), upload once,
+        // then one batched Householder launch for all modes.
+        int64_t total = 0;
+        for (int m = 0; m < N; m++) total += I[m] * R[m];
+        std::vector<double> h((size_t)total);
+        for (auto &v : h) v = libc_polar_randn();
+        DevMem a(ctx, total * sizeof(double));
+        DT_CUDA(cudaMemcpyAsync(a.get(), h.data(), total * sizeof(double), cudaMemcpyHostToDevice,
+                                ctx->stream));
+        std::vector<const double *> ap(N);
+        std::vector<double *> qp(N);
+        int64_t off = 0;
         for (int m = 0; m < N; m++) {
-            std::vector<double> h((size_t)(I[m] * R[m]));
-            for (auto &v : h) v = libc_polar_randn();
-            DevMem a(ctx, h.size() * sizeof(double));
-            DT_CUDA(cudaMemcpyAsync(a.get(), h.data(), h.size() * sizeof(double),
-                                    cudaMemcpyHostToDevice, ctx->stream));
-            DevMem w(ctx, (I[m] * R[m] + R[m]) * sizeof(double));
-            householder_qr(ctx, a.as<double>(), I[m], R[m], U[m].as<double>(), nullptr,
-                           w.as<double>());
-            DT_CUDA(cudaStreamSynchronize(ctx->stream));  // h goes out of scope
+            ap[m] = a.as<double>() + off;
+            qp[m] = U[m].as<double>();
+            off += I[m] * R[m];
         }
+        householder_qr_batch(ctx, N, ap.data(), qp.data(), I, R);
         return;
     }
     // HOSVD: leading R_n eigenvectors of X_(n) X_(n)^T by subspace iteration

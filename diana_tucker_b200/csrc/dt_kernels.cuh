@@ -39,6 +39,11 @@ void gemm_f64(dt_ctx *ctx, int transA, int transB, int64_t m, int64_t n, int64_t
 void householder_qr(dt_ctx *ctx, const double *A, int64_t m, int64_t n, double *Q,
                     double *R, double *work);
 
+// Householder QR of `count` matrices in one launch (one CTA each): Q[b] (m[b]
+// x n[b]) from A[b].  Host arrays of device pointers.
+void householder_qr_batch(dt_ctx *ctx, int count, const double *const *A, double *const *Q,
+                          const int64_t *m, const int64_t *n);
+
 // Orthonormal basis of span(S^iters L) for the n x n symmetric S and the n x r
 // col-major L (in place), one CTA; CholeskyQR2 per step with a Householder
 // fallback.  work >= 3*n*r + r.  Sets *flag bit 2 when a fallback ran.

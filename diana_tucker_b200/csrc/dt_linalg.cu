@@ -4,6 +4,8 @@
 // sweep never round-trips to the host.  These matrices are tiny (R x R, I_n x R,
 // I_n x I_n): one CTA per problem, latency-bound, so the code minimises block
 // barriers rather than flops.
+#include <vector>
+
 #include "dt_kernels.cuh"
 
 namespace dt {
@@ -122,7 +124,7 @@ __global__ void __launch_bounds__(LA_NT) hqr_kernel(const double *A, int64_t m, 
 // registers and rows are exchanged with shuffles, so the r pivots form one
 // short dependency chain (one sqrt and one reciprocal per pivot).  Returns
 // false on a non-positive pivot.  Runs in warp 0 only; r <= 32.
-template <int RMAX>
+template <int RMAX, bool INV = true>
 __device__ bool warp_chol_inv(double *G, double *Rinv, int r) {
     const int lane = threadIdx.x & 31;
     double g[RMAX], x[RMAX], invd[RMAX];
@@ -146,6 +148,15 @@ __device__ bool warp_chol_inv(double *G, double *Rinv, int r) {
             const double rki = __shfl_sync(0xffffffffu, g[k], i);
             if (lane >= i) g[i] = fma(-rki, g[k], g[i]);
         }
+    }
+    if (!INV) {
+        if (lane < r) {
+#pragma unroll
+            for (int i = 0; i < RMAX; i++)
+                if (i < r) G[i * r + lane] = i <= lane ? g[i] : 0.0;
+        }
+        __syncwarp();
+        return ok;
     }
     // Column `lane` of R^{-1} by back substitution; x[j] = 0 for j > lane.
 #pragma unroll
@@ -192,6 +203,28 @@ __device__ __forceinline__ double s_at(const double *S, int64_t n, int mode, int
     return S[i + n * k];
 }
 
+// Forward substitution Q[i, :] = Z[i, :] R^{-1} for every row i (R upper,
+// row-major r x r in smem, Rinv_diag its reciprocal diagonal), one thread per
+// row: the r-step chain runs on 96+ rows at once instead of one warp.
+__device__ __forceinline__ void rows_trsm(const double *Z, double *Q, int64_t n, int64_t r,
+                                          const double *R) {
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        double q[32];
+#pragma unroll
+        for (int c = 0; c < 32; c++) {
+            if (c >= r) break;
+            double acc = Z[i + c * n];
+#pragma unroll
+            for (int k = 0; k < 32; k++) {
+                if (k >= c) break;
+                acc = fma(-q[k], R[k * r + c], acc);
+            }
+            q[c] = acc / R[c * r + c];
+            Q[i + c * n] = q[c];
+        }
+    }
+}
+
 template <int RMAX>
 __global__ void __launch_bounds__(LA_NT) subspace_kernel(const double *Sg, int64_t n,
                                                          double *Lg, int64_t r, int iters,
@@ -202,7 +235,7 @@ __global__ void __launch_bounds__(LA_NT) subspace_kernel(const double *Sg, int64
     __shared__ int bad;
     const int t = threadIdx.x;
     double *G = sm;                // r*r
-    double *Ri = sm + r * r;       // r*r
+    double *Ri = sm + r * r;       // r*r (unused scratch for the Cholesky helper)
     double *cur = sm + 2 * r * r;  // after the two r x r blocks
     const double *S = Sg;
     if (s_mode == S_FULL) {
@@ -233,12 +266,51 @@ __global__ void __launch_bounds__(LA_NT) subspace_kernel(const double *Sg, int64
     __syncthreads();
     const int64_t cgroups = (r + 3) / 4;
     const int npairs = (int)(r * (r + 1) / 2);
-    for (int it = 0; it < iters; it++) {
-        // Z = S L; each task is one row i and four columns.
+
+    // One CholeskyQR pass: dst = orth(src) through G = src^T src = R^T R.
+    auto cholqr = [&](const double *src, double *dst) -> bool {
+        for (int task = t; task < 4 * ((npairs + 7) / 8) * 8; task += blockDim.x) {
+            const int pr = task >> 2, part = task & 3;
+            double sacc = 0.0;
+            int a = 0, b = 0;
+            if (pr < npairs) {
+                int rem = pr;
+                while (rem >= (int)r - a) {
+                    rem -= (int)r - a;
+                    a++;
+                }
+                b = a + rem;
+                const double *ca = src + (int64_t)a * n, *cb = src + (int64_t)b * n;
+                for (int64_t k = part; k < n; k += 4) sacc = fma(ca[k], cb[k], sacc);
+            }
+            sacc += __shfl_xor_sync(0xffffffffu, sacc, 1);
+            sacc += __shfl_xor_sync(0xffffffffu, sacc, 2);
+            if (pr < npairs && part == 0) {
+                G[a * r + b] = sacc;
+                G[b * r + a] = sacc;
+            }
+        }
+        __syncthreads();
+        if (t < 32) {
+            const bool ok = warp_chol_inv<RMAX, false>(G, Ri, (int)r);
+            if (t == 0) bad = ok ? 0 : 1;
+        }
+        __syncthreads();
+        if (bad) return false;
+        rows_trsm(src, dst, n, r, G);
+        __syncthreads();
+        return true;
+    };
+
+    // span(S^iters L): products Z <- S Z, orthonormalised after the second
+    // product (conditioning stays within (l1/lr)^2) and at the end (two passes).
+    bool broke = false;
+    double *cur_in = L, *cur_out = Z;
+    for (int it = 0; it < iters && !broke; it++) {
         for (int64_t task = t; task < n * cgroups; task += blockDim.x) {
             const int64_t i = task % n, c0 = 4 * (task / n);
             double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-            const double *l0 = L + c0 * n;
+            const double *l0 = cur_in + c0 * n;
             const bool h1 = c0 + 1 < r, h2 = c0 + 2 < r, h3 = c0 + 3 < r;
 #pragma unroll 4
             for (int64_t k = 0; k < n; k++) {
@@ -248,72 +320,55 @@ __global__ void __launch_bounds__(LA_NT) subspace_kernel(const double *Sg, int64
                 if (h2) a2 = fma(sv, l0[k + 2 * n], a2);
                 if (h3) a3 = fma(sv, l0[k + 3 * n], a3);
             }
-            Z[i + c0 * n] = a0;
-            if (h1) Z[i + (c0 + 1) * n] = a1;
-            if (h2) Z[i + (c0 + 2) * n] = a2;
-            if (h3) Z[i + (c0 + 3) * n] = a3;
+            cur_out[i + c0 * n] = a0;
+            if (h1) cur_out[i + (c0 + 1) * n] = a1;
+            if (h2) cur_out[i + (c0 + 2) * n] = a2;
+            if (h3) cur_out[i + (c0 + 3) * n] = a3;
         }
         __syncthreads();
-        bool broke = false;
-        const int passes = (it == iters - 1) ? 2 : 1;
-        for (int pass = 0; pass < passes && !broke; pass++) {
-            double *src = pass == 0 ? Z : L;
-            double *dst = pass == 0 ? L : Z;
-            // G = src^T src: four threads per (a, b) pair, strided over rows.
-            for (int task = t; task < 4 * ((npairs + 7) / 8) * 8; task += blockDim.x) {
-                const int pr = task >> 2, part = task & 3;
-                double sacc = 0.0;
-                int a = 0, b = 0;
-                if (pr < npairs) {
-                    // pr -> (a, b) with a <= b, row-major over the upper triangle.
-                    int rem = pr;
-                    a = 0;
-                    while (rem >= (int)r - a) {
-                        rem -= (int)r - a;
-                        a++;
-                    }
-                    b = a + rem;
-                    const double *ca = src + (int64_t)a * n, *cb = src + (int64_t)b * n;
-                    for (int64_t k = part; k < n; k += 4) sacc = fma(ca[k], cb[k], sacc);
-                }
-                sacc += __shfl_xor_sync(0xffffffffu, sacc, 1);
-                sacc += __shfl_xor_sync(0xffffffffu, sacc, 2);
-                if (pr < npairs && part == 0) {
-                    G[a * r + b] = sacc;
-                    G[b * r + a] = sacc;
-                }
-            }
-            __syncthreads();
-            if (t < 32) {
-                const bool ok = warp_chol_inv<RMAX>(G, Ri, (int)r);
-                if (t == 0) bad = ok ? 0 : 1;
-            }
-            __syncthreads();
-            if (bad) {
+        double *tmp = cur_in;
+        cur_in = cur_out;
+        cur_out = tmp;
+        const bool last = it == iters - 1;
+        if (last || (it % 2) == 1) {
+            // cur_in holds the product; orthonormalise into cur_out, then back.
+            if (!cholqr(cur_in, cur_out)) {
                 broke = true;
                 break;
             }
-            for (int64_t e = t; e < n * r; e += blockDim.x) {
-                const int64_t i = e % n, c = e / n;
-                double sacc = 0.0;
-                for (int64_t k = 0; k <= c; k++) sacc = fma(src[i + k * n], Ri[k * r + c], sacc);
-                dst[e] = sacc;
+            if (last) {
+                if (!cholqr(cur_out, cur_in)) {
+                    broke = true;
+                    break;
+                }
+            } else {
+                tmp = cur_in;
+                cur_in = cur_out;
+                cur_out = tmp;
             }
-            __syncthreads();
-        }
-        if (broke) {
-            // Householder on S L (Z holds it whichever pass broke).
-            for (int64_t e = t; e < n * r; e += blockDim.x) hwork[e] = Z[e];
-            __syncthreads();
-            hqr_device(hwork, n, r, hwork + n * r, L, red);
-            if (t == 0 && flag) atomicOr(flag, 2);
-            __syncthreads();
-        } else if (passes == 2) {
-            for (int64_t e = t; e < n * r; e += blockDim.x) L[e] = Z[e];
-            __syncthreads();
         }
     }
-    for (int64_t e = t; e < n * r; e += blockDim.x) Lg[e] = L[e];
+    if (broke) {
+        // Rank-deficient or badly conditioned: restart from the caller's L and
+        // run every step with Householder orthonormalisation.
+        for (int64_t e = t; e < n * r; e += blockDim.x) L[e] = Lg[e];
+        __syncthreads();
+        for (int it = 0; it < iters; it++) {
+            for (int64_t e = t; e < n * r; e += blockDim.x) {
+                const int64_t i = e % n, c = e / n;
+                double acc = 0.0;
+                for (int64_t k = 0; k < n; k++) acc = fma(s_at(S, n, s_mode, i, k), L[k + c * n], acc);
+                hwork[e] = acc;
+            }
+            __syncthreads();
+            hqr_device(hwork, n, r, hwork + n * r, L, red);
+            __syncthreads();
+        }
+        if (t == 0 && flag) atomicOr(flag, 2);
+        for (int64_t e = t; e < n * r; e += blockDim.x) Lg[e] = L[e];
+        return;
+    }
+    for (int64_t e = t; e < n * r; e += blockDim.x) Lg[e] = cur_in[e];
 }
 
 // Subspace iteration for ranks above 32: Householder QR every step, S, L and Z
@@ -425,6 +480,20 @@ __global__ void __launch_bounds__(LA_NT) lu_inverse_kernel(const double *A, int6
     }
 }
 
+// Householder QR of several small matrices at once (one CTA each, 128
+// threads so the per-column barriers stay cheap): Q[b] = Q of A[b].
+__global__ void __launch_bounds__(128) hqr_batch_kernel(const double *const *A,
+                                                         double *const *Q, const int64_t *m,
+                                                         const int64_t *n, double *const *work) {
+    __shared__ double red[33];
+    const int b = blockIdx.x;
+    const int64_t mb = m[b], nb = n[b];
+    double *W = work[b];
+    for (int64_t e = threadIdx.x; e < mb * nb; e += blockDim.x) W[e] = A[b][e];
+    __syncthreads();
+    hqr_device(W, mb, nb, W + mb * nb, Q[b], red);
+}
+
 // Cholesky of the r x r SPD G (col-major) and L^{-1} (lower) for the row
 // orthonormalisation; one CTA, r small.  Output Linv col-major.
 __global__ void chol_lower_inv_kernel(const double *Gg, int r, double *Linv, int *flag) {
@@ -516,6 +585,36 @@ void householder_qr(dt_ctx *ctx, const double *A, int64_t m, int64_t n, double *
     DT_CHECK_ARG(m >= n && n > 0, "householder_qr: need m >= n > 0 (m=%lld n=%lld)",
                  (long long)m, (long long)n);
     DT_LAUNCH(ctx, hqr_kernel, 1, LA_NT, 0, A, m, n, Q, R, work);
+}
+
+void householder_qr_batch(dt_ctx *ctx, int count, const double *const *A, double *const *Q,
+                          const int64_t *m, const int64_t *n) {
+    // Pointer and size tables plus per-matrix workspaces, staged to the device.
+    std::vector<const double *> hA(A, A + count);
+    std::vector<double *> hQ(Q, Q + count), hW(count);
+    std::vector<int64_t> hm(m, m + count), hn(n, n + count);
+    std::vector<DevMem> ws(count);
+    for (int b = 0; b < count; b++) {
+        DT_CHECK_ARG(m[b] >= n[b] && n[b] > 0, "householder_qr_batch: need m >= n > 0");
+        ws[b].alloc(ctx, (m[b] * n[b] + n[b]) * sizeof(double));
+        hW[b] = ws[b].as<double>();
+    }
+    DevMem tab(ctx, count * (3 * sizeof(void *) + 2 * sizeof(int64_t)));
+    char *base = static_cast<char *>(tab.get());
+    const size_t pb = count * sizeof(void *);
+    DT_CUDA(cudaMemcpyAsync(base, hA.data(), pb, cudaMemcpyHostToDevice, ctx->stream));
+    DT_CUDA(cudaMemcpyAsync(base + pb, hQ.data(), pb, cudaMemcpyHostToDevice, ctx->stream));
+    DT_CUDA(cudaMemcpyAsync(base + 2 * pb, hW.data(), pb, cudaMemcpyHostToDevice, ctx->stream));
+    DT_CUDA(cudaMemcpyAsync(base + 3 * pb, hm.data(), count * sizeof(int64_t),
+                            cudaMemcpyHostToDevice, ctx->stream));
+    DT_CUDA(cudaMemcpyAsync(base + 3 * pb + count * sizeof(int64_t), hn.data(),
+                            count * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
+    DT_LAUNCH(ctx, hqr_batch_kernel, count, 128, 0, reinterpret_cast<const double *const *>(base),
+              reinterpret_cast<double *const *>(base + pb),
+              reinterpret_cast<const int64_t *>(base + 3 * pb),
+              reinterpret_cast<const int64_t *>(base + 3 * pb + count * sizeof(int64_t)),
+              reinterpret_cast<double *const *>(base + 2 * pb));
+    DT_CUDA(cudaStreamSynchronize(ctx->stream));  // host tables go out of scope
 }
 
 void subspace_iter(dt_ctx *ctx, const double *S, int64_t n, double *L, int64_t r, int iters,

@@ -30,7 +30,8 @@ namespace {
 
 using namespace tc;
 
-constexpr int TTM_THREADS = 192;
+constexpr int TTM_EPI_WARPS = 8;
+constexpr int TTM_THREADS = 64 + 32 * TTM_EPI_WARPS;  // TMA warp, MMA warp, epilogue
 constexpr int KC_ELEMS = 64;         // BF16 elements per 128-byte row
 constexpr int KC_BYTES = 128 * 128;  // one 128-row x 128-byte K-chunk of A
 
@@ -61,17 +62,31 @@ __device__ __forceinline__ int64_t out_rowbase(const OutMap &om, int64_t lp, int
 // ---------------------------------------------------------------------------
 // TTM
 // ---------------------------------------------------------------------------
+template <int JH>
+__device__ __forceinline__ void tmem_ld_half(uint32_t taddr, float (&v)[JH]) {
+    if constexpr (JH == 8) {
+        tmem_ld8(taddr, v);
+    } else {
+        tmem_ld16(taddr, v);
+    }
+}
+
+// JP: padded output width (16 or 32); SPLIT: hi+lo operands; FOLDED: the
+// output is the folded tensor Y[l, j, b] (else a general OutMap).
+template <int JP, bool SPLIT, bool FOLDED>
 __global__ void __launch_bounds__(TTM_THREADS, 1)
     tc_ttm_kernel(const __grid_constant__ CUtensorMap map_hi,
                   const __grid_constant__ CUtensorMap map_lo, const TcTtmArgs a) {
+    constexpr int NPAD = SPLIT ? 2 * JP : JP;
+    constexpr int JH = JP / 2;  // columns per epilogue warp
     extern __shared__ uint8_t smem_raw[];
     uint8_t *sm = align1024(smem_raw);
     const int S = a.stages;
-    uint8_t *Bt = sm;                                   // kchunks x Npad rows x 128 B
-    const uint32_t b_bytes = (uint32_t)a.kchunks * a.Npad * 128;
+    uint8_t *Bt = sm;                                   // kchunks x NPAD rows x 128 B
+    const uint32_t b_bytes = (uint32_t)a.kchunks * NPAD * 128;
     uint8_t *Abase = sm + ((b_bytes + 1023) & ~1023u);  // stages
     const uint32_t a_one = (uint32_t)a.kchunks * KC_BYTES;
-    const uint32_t stage_bytes = a_one * (a.split ? 2 : 1);
+    const uint32_t stage_bytes = a_one * (SPLIT ? 2 : 1);
     uint64_t *bars = reinterpret_cast<uint64_t *>(Abase + (size_t)S * stage_bytes);
     uint64_t *full = bars, *empty = bars + S, *tfull = bars + 2 * S, *tempty = bars + 2 * S + 2;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * S + 4);
@@ -88,25 +103,23 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
         }
         for (int i = 0; i < 2; i++) {
             mbar_init(&tfull[i], 1);
-            mbar_init(&tempty[i], 128);
+            mbar_init(&tempty[i], TTM_EPI_WARPS * 32);
         }
         fence_mbar_init();
     }
     // B = [U_hi | U_lo]^T (split) or U_hi^T, K-major, 128B-swizzled, zero padded.
     {
-        const int Jp = a.Jpad;
-        const int nrows = a.Npad;
         const int kmax = a.kchunks * KC_ELEMS;
-        for (int e = threadIdx.x; e < nrows * kmax; e += blockDim.x) {
+        for (int e = threadIdx.x; e < NPAD * kmax; e += blockDim.x) {
             const int row = e / kmax, k = e - row * kmax;
-            const int j = row % Jp;
-            const bool lo_part = row >= Jp;
+            const int j = row % JP;
+            const bool lo_part = row >= JP;
             float v = 0.f;
             if (j < a.J && k < a.I) v = (float)a.U[(int64_t)k + (int64_t)a.I * j];
             __nv_bfloat16 hi, lo;
             bf16_split(v, hi, lo);
             const int kc = k / KC_ELEMS, kk = k - kc * KC_ELEMS;
-            uint8_t *dst = Bt + (uint32_t)kc * nrows * 128 + sw128_kmajor_offset(row, kk);
+            uint8_t *dst = Bt + (uint32_t)kc * NPAD * 128 + sw128_kmajor_offset(row, kk);
             *reinterpret_cast<__nv_bfloat16 *>(dst) = lo_part ? lo : hi;
         }
     }
@@ -119,7 +132,7 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
     if (warp == 0) {
         if (lane == 0) {
             prefetch_tmap(&map_hi);
-            if (a.split) prefetch_tmap(&map_lo);
+            if (SPLIT) prefetch_tmap(&map_lo);
             int64_t k = 0;
             bool ok = true;
             for (int64_t tile = blockIdx.x; tile < a.ntiles && ok; tile += gridDim.x, k++) {
@@ -132,7 +145,7 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
                     const int r0 = (int)(tile * 128);
                     for (int kc = 0; kc < a.kchunks; kc++) {
                         tma_load_2d(st + kc * KC_BYTES, &map_hi, &full[s], kc * KC_ELEMS, r0);
-                        if (a.split)
+                        if (SPLIT)
                             tma_load_2d(st + a_one + kc * KC_BYTES, &map_lo, &full[s],
                                         kc * KC_ELEMS, r0);
                     }
@@ -143,7 +156,7 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
                         for (int h = 0; h < 2; h++) {
                             uint8_t *d = st + kc * KC_BYTES + h * (KC_BYTES / 2);
                             tma_load_3d(d, &map_hi, &full[s], l0 + h * 64, kc * KC_ELEMS, (int)b);
-                            if (a.split)
+                            if (SPLIT)
                                 tma_load_3d(d + a_one, &map_lo, &full[s], l0 + h * 64,
                                             kc * KC_ELEMS, (int)b);
                         }
@@ -151,13 +164,13 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
             }
             // Leave no copy in flight: wait (bounded) for every stage issued.
             const int64_t issued = k;
-            for (int64_t q = std::max<int64_t>(0, issued - S); q < issued; q++)
+            for (int64_t q = issued - S > 0 ? issued - S : 0; q < issued; q++)
                 mbar_wait(&full[q % S], (uint32_t)((q / S) & 1), a.err);
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            const uint32_t id_full = idesc_bf16(128, a.Npad, !a.kmajor, false);
-            const uint32_t id_half = idesc_bf16(128, a.Jpad, !a.kmajor, false);
+            const uint32_t id_full = idesc_bf16(128, NPAD, !a.kmajor, false);
+            const uint32_t id_half = idesc_bf16(128, JP, !a.kmajor, false);
             int64_t k = 0;
             bool ok = true;
             for (int64_t tile = blockIdx.x; tile < a.ntiles && ok; tile += gridDim.x, k++) {
@@ -167,7 +180,7 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
                 if (ok && k >= 2) ok = mbar_wait(&tempty[acc], (uint32_t)(((k / 2) - 1) & 1), a.err);
                 if (!ok) break;
                 tc_fence_after();
-                const uint32_t d = tmem_base + (uint32_t)(acc * a.Npad);
+                const uint32_t d = tmem_base + (uint32_t)(acc * NPAD);
                 const uint32_t st = smem_u32(Abase + (size_t)s * stage_bytes);
                 const uint32_t bt = smem_u32(Bt);
                 for (int ks = 0; ks < a.ksteps; ks++) {
@@ -182,46 +195,46 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
                                     kSwizzle128B);
                     }
                     const uint64_t bd =
-                        sdesc(bt + (uint32_t)kc * a.Npad * 128 + sub * 32, 16, 1024, kSwizzle128B);
+                        sdesc(bt + (uint32_t)kc * NPAD * 128 + sub * 32, 16, 1024, kSwizzle128B);
                     umma_bf16(d, ad, bd, id_full, ks > 0 ? 1u : 0u);
-                    if (a.split) umma_bf16(d, adl, bd, id_half, 1u);
+                    if (SPLIT) umma_bf16(d, adl, bd, id_half, 1u);
                 }
                 umma_commit(&empty[s]);
                 umma_commit(&tfull[acc]);
             }
             // Drain: the last two accumulators' MMAs must finish before dealloc.
             const int64_t issued = k;
-            for (int64_t q = std::max<int64_t>(0, issued - 2); q < issued; q++)
+            for (int64_t q = issued - 2 > 0 ? issued - 2 : 0; q < issued; q++)
                 mbar_wait(&tfull[q & 1], (uint32_t)((q / 2) & 1), a.err);
         }
     } else {
-        // Epilogue warps 2..5 -> TMEM lane quarters 2, 3, 0, 1.
+        // Epilogue warps 2..9: two per TMEM lane quarter, each half of the columns.
+        const int e = warp - 2;
         const int quarter = warp & 3;
+        const int half = e >> 2;
         const int m = quarter * 32 + lane;
+        const int j0 = half * JH;
+        const int64_t LJ = a.L * a.J;
         int64_t k = 0;
         for (int64_t tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x, k++) {
             const int acc = (int)(k & 1);
             if (!mbar_wait(&tfull[acc], (uint32_t)((k / 2) & 1), a.err)) break;
             tc_fence_after();
-            const uint32_t taddr = tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * a.Npad);
-            float v[64];
+            const uint32_t taddr =
+                tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * NPAD + j0);
+            float v[JH];
+            tmem_ld_half<JH>(taddr, v);
+            if (SPLIT) {
+                float w[JH];
+                tmem_ld_half<JH>(taddr + JP, w);
+                tmem_wait_ld();
 #pragma unroll
-            for (int g = 0; g < 4; g++) {
-                if (g * 16 < a.Npad) {
-                    float tmp[16];
-                    tmem_ld16(taddr + g * 16, tmp);
-#pragma unroll
-                    for (int i = 0; i < 16; i++) v[g * 16 + i] = tmp[i];
-                }
+                for (int j = 0; j < JH; j++) v[j] += w[j];
+            } else {
+                tmem_wait_ld();
             }
-            tmem_wait_ld();
             tc_fence_before();
             mbar_arrive(&tempty[acc]);
-            if (a.split) {
-#pragma unroll
-                for (int j = 0; j < 32; j++)
-                    if (j < a.Jpad) v[j] += v[a.Jpad + j];
-            }
             int64_t lp, bp;
             bool valid;
             if (a.kmajor) {
@@ -235,19 +248,39 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
                 valid = lp < a.L;
             }
             if (!valid) continue;
-            const int64_t base = out_rowbase(a.om, lp, bp);
+            int64_t base, js;
+            if (FOLDED) {
+                base = lp + bp * LJ;
+                js = a.L;
+            } else {
+                base = out_rowbase(a.om, lp, bp);
+                js = a.om.jstride;
+            }
             if (a.out_f32) {
 #pragma unroll
-                for (int j = 0; j < 32; j++)
-                    if (j < a.J) a.out_f32[base + j * a.om.jstride] = v[j];
+                for (int j = 0; j < JH; j++)
+                    if (j0 + j < a.J) a.out_f32[base + (j0 + j) * js] = v[j];
+            } else if (FOLDED && js == 1 && (a.J % JP) == 0) {
+                // Contiguous row segment: 16-byte stores.
+                __nv_bfloat16 hi[JH], lo[JH];
+#pragma unroll
+                for (int j = 0; j < JH; j++) bf16_split(v[j], hi[j], lo[j]);
+                uint4 *dh = reinterpret_cast<uint4 *>(a.out_hi + base + j0);
+#pragma unroll
+                for (int q = 0; q < JH / 8; q++) dh[q] = reinterpret_cast<const uint4 *>(hi)[q];
+                if (a.out_lo) {
+                    uint4 *dl = reinterpret_cast<uint4 *>(a.out_lo + base + j0);
+#pragma unroll
+                    for (int q = 0; q < JH / 8; q++) dl[q] = reinterpret_cast<const uint4 *>(lo)[q];
+                }
             } else {
 #pragma unroll
-                for (int j = 0; j < 32; j++) {
-                    if (j < a.J) {
+                for (int j = 0; j < JH; j++) {
+                    if (j0 + j < a.J) {
                         __nv_bfloat16 hi, lo;
                         bf16_split(v[j], hi, lo);
-                        a.out_hi[base + j * a.om.jstride] = hi;
-                        if (a.out_lo) a.out_lo[base + j * a.om.jstride] = lo;
+                        a.out_hi[base + (j0 + j) * js] = hi;
+                        if (a.out_lo) a.out_lo[base + (j0 + j) * js] = lo;
                     }
                 }
             }
@@ -564,10 +597,21 @@ void tc_ttm(dt_ctx *ctx, const __nv_bfloat16 *Xh, const __nv_bfloat16 *Xl, int64
         ml = Xl ? make_map(Xl, 3, dims, str, box) : mh;
     }
     const size_t smem = 1024 + b_bytes + (size_t)S * stage_bytes + (2 * S + 4) * 8 + 16;
-    DT_CUDA(cudaFuncSetAttribute(tc_ttm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
     const unsigned grid = (unsigned)std::min<int64_t>(a.ntiles, ctx->num_sms);
-    DT_LAUNCH(ctx, tc_ttm_kernel, grid, TTM_THREADS, smem, mh, ml, a);
+    const bool folded = om.nl == 1 && om.nb == 1 && om.dl[0] == std::max<int64_t>(L, 1) &&
+                        om.sl[0] == 1 && om.sb[0] == L * J && om.jstride == L;
+    auto go = [&](auto kernel) {
+        DT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+        DT_LAUNCH(ctx, kernel, grid, TTM_THREADS, smem, mh, ml, a);
+    };
+    if (a.Jpad == 16) {
+        if (a.split) folded ? go(tc_ttm_kernel<16, true, true>) : go(tc_ttm_kernel<16, true, false>);
+        else folded ? go(tc_ttm_kernel<16, false, true>) : go(tc_ttm_kernel<16, false, false>);
+    } else {
+        if (a.split) folded ? go(tc_ttm_kernel<32, true, true>) : go(tc_ttm_kernel<32, true, false>);
+        else folded ? go(tc_ttm_kernel<32, false, true>) : go(tc_ttm_kernel<32, false, false>);
+    }
 }
 
 bool tc_gram_supported(int64_t I, int64_t K) {

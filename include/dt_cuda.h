@@ -51,6 +51,7 @@ extern "C" {
                                 (hooi_als.tpp:74-81, util.cpp:10-18) */
 #define DT_INIT_HOSVD 1      /* leading R_n eigenvectors of X_(n) X_(n)^T */
 #define DT_INIT_GIVEN 2      /* factors supplied by the caller in U */
+#define DT_SEED_KEEP 0xFFFFFFFFu
 
 /* HOOI arithmetic for the TTM chain and the Gram (the eigensolve / QR, the
  * fit and the final core projection are FP64 in every mode). */
@@ -62,7 +63,9 @@ typedef struct dt_ctx dt_ctx;
 
 typedef struct {
     int init;           /* DT_INIT_* */
-    unsigned seed;      /* for DT_INIT_RANDN_LIBC */
+    unsigned seed;      /* for DT_INIT_RANDN_LIBC: srand(seed) first; DT_SEED_KEEP
+                           continues the process's current rand() sequence, as
+                           the reference's HOOI_ALS does after the caller's srand */
     int max_sweeps;     /* reference: max_iter */
     double tol;         /* stop when |res_k - res_{k-1}| < tol; <= 0 runs max_sweeps */
     int inner_iters;    /* subspace iterations per mode (reference ALS_: 5) */
@@ -185,6 +188,31 @@ DT_API int dt_hooi_dense(dt_ctx *ctx, const void *X, int dtype, int ndim, const 
 /* Fills opts with the reference's behaviour: random libc init, 5 inner
  * iterations, FP64, no tolerance. */
 DT_API void dt_hooi_default_opts(dt_hooi_opts *opts);
+
+/* ---- batched dense HOOI ------------------------------------------------ */
+typedef struct {
+    double device_ms;    /* CUDA-event time of the graph launch */
+    int block_threads;   /* block size used (autotuned when 0 was requested) */
+    int grid;            /* persistent CTAs (resident CTAs per SM x SMs) */
+    int kernel_launches;
+    double tune_ms[3];   /* autotuner timings of 128 / 256 / 512 threads (0 if cached) */
+} dt_batched_report;
+
+/* HOOI of `count` independent 3-way tensors in one persistent launch (CUDA
+ * graph: queue reset + kernel).  Tensor t has shape shapes[3t..3t+2] (each
+ * <= 64), ranks ranks[3t..3t+2] (each <= 8 and <= the mode size), FP32 data
+ * at X + x_offsets[t] (column-major), initial factors (I_n x R_n col-major,
+ * FP64) at U + u_offsets[3t+n], overwritten with the result; the core goes to
+ * G + g_offsets[t] and the relative error sqrt(1 - ||G||^2/||X||^2) to
+ * relerr[t].  `sweeps` HOOI sweeps with `inner_iters` ALS_ steps per mode, in
+ * FP64.  block_threads = 0 autotunes the block size on a sample of the batch
+ * (cached per batch signature).  Batched form of Algorithm::Tucker::HOOI_ALS
+ * (hooi_als.tpp:64-123); no reference counterpart for the batching. */
+DT_API int dt_hooi_batched(dt_ctx *ctx, int count, const int64_t *shapes, const int64_t *ranks,
+                           const float *X, const int64_t *x_offsets, int sweeps, int inner_iters,
+                           double *U, const int64_t *u_offsets, double *G,
+                           const int64_t *g_offsets, double *relerr, int block_threads,
+                           dt_batched_report *report);
 
 /* ---- sparse tensors --------------------------------------------------- */
 typedef struct dt_sptensor dt_sptensor;
