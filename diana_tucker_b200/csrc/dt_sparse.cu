@@ -399,7 +399,7 @@ void launch_rows(dt_ctx *ctx, const ModeCopy &mc, int nother, int64_t nnz, const
 
 // Compact Y_(n): Yc is nrows x P row-major (row k = mode-n row mc.rows[k]).
 void sp_ttmc_compact(dt_ctx *ctx, const dt_sptensor *sp, const double *const *Ut_dev,
-                     const int64_t *R, int mode, double *Yc) {
+                     const int64_t *R, int mode, double *Yc, LaunchTimer *timer = nullptr) {
     const ModeCopy &mc = sp->modes[mode];
     const int nd = sp->ndim;
     const int64_t P64 = kron_len(R, nd, mode);
@@ -415,6 +415,7 @@ void sp_ttmc_compact(dt_ctx *ctx, const dt_sptensor *sp, const double *const *Ut
         d++;
     }
     DevMem part(ctx, std::max<int64_t>(mc.nslots, 1) * P * sizeof(double));
+    if (timer) timer->begin();
     const bool fast3 = nd == 3 && f.R[0] <= 32 && (32 % f.R[0]) == 0 && f.R[1] <= 32;
     const int PL = (P + 31) / 32;
     if (fast3) {
@@ -437,6 +438,15 @@ void sp_ttmc_compact(dt_ctx *ctx, const dt_sptensor *sp, const double *const *Ut
         DT_LAUNCH(ctx, combine_partials_kernel, blocks, 256, 0, part.as<double>(),
                   mc.multi_row.as<int32_t>(), mc.multi_first.as<int32_t>(),
                   mc.multi_count.as<int32_t>(), mc.nmulti, P, Yc);
+    }
+    if (timer) {
+        // Algorithmic bytes of the TTMc: the mode-sorted nonzeros (int32 indices
+        // of the other modes + FP64 value), each other factor read once, and
+        // the compact Y_(n) rows written.
+        double bytes = (double)sp->nnz * (4.0 * (nd - 1) + 8.0) + (double)mc.nrows * P * 8.0;
+        for (int m = 0; m < nd; m++)
+            if (m != mode) bytes += (double)sp->shape[m] * R[m] * 8.0;
+        timer->end(bytes);
     }
 }
 
@@ -657,11 +667,12 @@ int dt_sp_hooi(dt_ctx *ctx, const dt_sptensor *sp, const int64_t *R, int max_swe
             maxYc = std::max<int64_t>(maxYc, sp->modes[m].nrows * kron_len(R, nd, m));
         DevMem Yc(ctx, maxYc * sizeof(double));
         DevMem L(ctx, 1024 * 32 * sizeof(double));
+        LaunchTimer timer(ctx, true);  // TTMc launches, reported as ttm_x_*
         DT_CUDA(cudaEventRecord(ctx->ev_start, ctx->stream));
         for (int it = 0; it < max_sweeps; it++) {
             for (int n = 0; n < nd; n++) {
                 const int P = (int)kron_len(R, nd, n);
-                sp_ttmc_compact(ctx, sp, ptrs, R, n, Yc.as<double>());
+                sp_ttmc_compact(ctx, sp, ptrs, R, n, Yc.as<double>(), &timer);
                 sp_mtr(ctx, sp, Yc.as<double>(), n, P, ptrs[n], (int)R[n], L.as<double>());
                 sp_mtl(ctx, sp, Yc.as<double>(), n, P, L.as<double>(), (int)R[n],
                        const_cast<double *>(ptrs[n]));
@@ -696,6 +707,10 @@ int dt_sp_hooi(dt_ctx *ctx, const dt_sptensor *sp, const int64_t *R, int max_swe
                 std::sqrt(std::max(0.0, 1.0 - hg2 / (sp->fnorm * sp->fnorm)));
             report->device_ms = ms;
             report->kernel_launches = (int)(ctx->launches - launches0);
+            report->precision_used = DT_PREC_FP64;
+            report->ttm_x_launches = timer.count();
+            report->ttm_x_ms = timer.total_ms();
+            report->ttm_x_bytes = timer.bytes();
         }
     });
 }

@@ -122,12 +122,19 @@ def random_orthonormal_transposed(shape, ranks, seed):
 
 def batched_small(count=4096, seed=3, lo=8, hi=64, rlo=2, rhi=8, noise_var=1e-4):
     """`count` 3-way FP32 Tucker tensors, modes ~ U[lo, hi], ranks ~ U[rlo, rhi]
-    capped at the mode size.  Returns a list of (X, ranks)."""
+    capped at the mode size and at the product of the other two ranks.
+    Returns a list of (X, ranks)."""
     rng = np.random.default_rng(seed)
     out = []
     for _ in range(count):
         shape = tuple(int(v) for v in rng.integers(lo, hi + 1, size=3))
-        ranks = tuple(min(int(r), s) for r, s in zip(rng.integers(rlo, rhi + 1, size=3), shape))
+        ranks = [min(int(r), s) for r, s in zip(rng.integers(rlo, rhi + 1, size=3), shape)]
+        # A Tucker model needs R_n <= prod_{m != n} R_m (else the mode-n Gram
+        # has rank below R_n and the extra factor columns are arbitrary).
+        for n in range(3):
+            others = ranks[(n + 1) % 3] * ranks[(n + 2) % 3]
+            ranks[n] = min(ranks[n], others)
+        ranks = tuple(ranks)
         sub_seed = int(rng.integers(0, 2**31 - 1))
         X = tucker_dense(shape, ranks, noise_var=noise_var, seed=sub_seed, dtype=np.float32)
         out.append((X, ranks))

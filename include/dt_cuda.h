@@ -250,8 +250,9 @@ DT_API int dt_sp_ttmc_rows(dt_ctx *ctx, const dt_sptensor *sp, const double *con
 /* Sparse HOOI power sweeps: per mode L = Y_(n)^T U_n, U_n <- orth(Y_(n) L);
  * core G (P_{N-1} x R_{N-1} col-major = the core tensor col-major) after the
  * sweeps.  Ut holds the initial transposed factors on entry and the final
- * ones on exit.  Replaces Algorithm::SpTucker::Sp_HOOI_ALS
- * (sp_hooi_als.tpp:67-118). */
+ * ones on exit.  The report's ttm_x_* fields time the TTMc launches (CUDA
+ * events) with their algorithmic bytes.  Replaces
+ * Algorithm::SpTucker::Sp_HOOI_ALS (sp_hooi_als.tpp:67-118). */
 DT_API int dt_sp_hooi(dt_ctx *ctx, const dt_sptensor *sp, const int64_t *R, int max_sweeps,
                double *const *Ut, double *G, dt_hooi_report *report);
 
