@@ -139,6 +139,17 @@ class Context:
                                         _i64p(s), n, gb.ptr))
         return G
 
+    def gram_noalloc(self, X, n: int, G):
+        """gram() into a caller-provided G, allocating nothing
+        (dt_gram_f64_noalloc): X and G must be torch CUDA float64 tensors."""
+        if not (_is_torch(X) and _is_torch(G) and X.is_cuda and G.is_cuda):
+            raise TypeError("gram_noalloc needs torch CUDA tensors for X and G")
+        self._bind(X, G)
+        xb, gb = _Buf(X), _Buf(G)
+        s = _shape_arr(X.shape)
+        _lib.check(self.lib.dt_gram_f64_noalloc(self.h, xb.ptr, X.dim(), _i64p(s), n, gb.ptr))
+        return G
+
     def ttt_except(self, A, B, n: int):
         self._bind(A, B)
         ab, bb = _Buf(A), _Buf(B)

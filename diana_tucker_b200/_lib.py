@@ -103,6 +103,8 @@ _SIGS = [
     ("dt_ttm_f64", ctypes.c_int, [_vp, _vp, ctypes.c_int, c_i64p, ctypes.c_int, _vp,
                                   ctypes.c_int64, _vp]),
     ("dt_gram_f64", ctypes.c_int, [_vp, _vp, ctypes.c_int, c_i64p, ctypes.c_int, _vp]),
+    ("dt_gram_f64_noalloc", ctypes.c_int, [_vp, _vp, ctypes.c_int, c_i64p, ctypes.c_int,
+                                           _vp]),
     ("dt_ttt_except_f64", ctypes.c_int, [_vp, _vp, c_i64p, _vp, c_i64p, ctypes.c_int,
                                          ctypes.c_int, _vp]),
     ("dt_fnorm_f64", ctypes.c_int, [_vp, _vp, ctypes.c_int64, c_dp]),

@@ -536,6 +536,44 @@ void ttt_f64(dt_ctx *ctx, const double *A, const double *Bt, int64_t L, int64_t 
     gemm_generic(ctx, unfolding(A, L, IA), unfolding(Bt, L, IB), IA, IB, L * B, C, IA, 0.0);
 }
 
+void ttt_f64_scratch(dt_ctx *ctx, const double *A, const double *Bt, int64_t L, int64_t IA,
+                     int64_t IB, int64_t B, double *C, double *scratch, int64_t scratch_doubles) {
+    // Same tiles, split choice and reduction as gemm_generic, with the split-K
+    // partial tiles in the caller's scratch; the split count is lowered when
+    // nsplit * IA * IB doubles would not fit.
+    const int64_t M = IA, N = IB, K = L * B;
+    if (M == 0 || N == 0) return;
+    const int64_t MN = M * N;
+    DT_CHECK_ARG(MN <= scratch_doubles,
+                 "ttt_f64_scratch: %lld x %lld result needs more than %lld scratch doubles",
+                 (long long)M, (long long)N, (long long)scratch_doubles);
+    const Operand a = unfolding(A, L, IA), b = unfolding(Bt, L, IB);
+    const int64_t tiles = (int64_t)ceil_div(M, GM_B) * ceil_div(N, GM_B);
+    const int64_t target = 2LL * ctx->num_sms;
+    int64_t nsplit = 1;
+    if (tiles < target && K > 256) {
+        nsplit = (target + tiles - 1) / tiles;
+        nsplit = std::min<int64_t>(nsplit, (K + 127) / 128);
+        nsplit = std::min<int64_t>(nsplit, scratch_doubles / MN);
+        nsplit = std::max<int64_t>(nsplit, 1);
+    }
+    int64_t kchunk = (K + nsplit - 1) / nsplit;
+    kchunk = ((kchunk + GM_BK - 1) / GM_BK) * GM_BK;
+    if (kchunk == 0) kchunk = GM_BK;
+    nsplit = (K + kchunk - 1) / kchunk;
+    if (nsplit < 1) nsplit = 1;
+    dim3 grid(ceil_div(M, GM_B), ceil_div(N, GM_B), (unsigned)nsplit);
+    if (nsplit == 1) {
+        DT_LAUNCH(ctx, gemm_kernel, grid, GM_NT, 0, a, b, M, N, K, kchunk, C, M, 0.0,
+                  (double *)nullptr);
+    } else {
+        DT_LAUNCH(ctx, gemm_kernel, grid, GM_NT, 0, a, b, M, N, K, kchunk, C, M, 0.0, scratch);
+        const unsigned blocks = std::min<unsigned>(ceil_div(MN, 256), 4096u);
+        DT_LAUNCH(ctx, splitk_reduce_kernel, blocks, 256, 0, (const double *)scratch, (int)nsplit,
+                  M, N, C, M, 0.0);
+    }
+}
+
 void gemm_f64(dt_ctx *ctx, int transA, int transB, int64_t m, int64_t n, int64_t k,
               const double *A, int64_t lda, const double *B, int64_t ldb, double *C,
               int64_t ldc, double beta) {

@@ -22,6 +22,11 @@ void ttm_f64(dt_ctx *ctx, const TX *X, int64_t L, int64_t I, int64_t B, const do
 void ttt_f64(dt_ctx *ctx, const double *A, const double *Bt, int64_t L, int64_t IA,
              int64_t IB, int64_t B, double *C);
 
+// ttt_f64 with the split-K partial tiles in caller-provided device scratch of
+// scratch_doubles doubles (>= IA * IB); allocates nothing.
+void ttt_f64_scratch(dt_ctx *ctx, const double *A, const double *Bt, int64_t L, int64_t IA,
+                     int64_t IB, int64_t B, double *C, double *scratch, int64_t scratch_doubles);
+
 // out[0] = sum x[e]^2 (deterministic two-stage reduction).  dtype DT_F64/DT_F32.
 void sumsq(dt_ctx *ctx, const void *x, int dtype, int64_t n, double *out);
 

@@ -120,6 +120,18 @@ DT_API int dt_ttm_f64(dt_ctx *ctx, const double *X, int ndim, const int64_t *sha
 DT_API int dt_gram_f64(dt_ctx *ctx, const double *X, int ndim, const int64_t *shape, int mode,
                 double *G);
 
+/* dt_gram_f64 without allocating: no counterpart in the reference.  For
+ * callers that cannot call cudaMalloc while they run (a host framework that
+ * owns the device heap, a latency-critical path where an allocation may
+ * synchronise or fail).  X and G must be device memory of the context's GPU;
+ * shape[mode] <= 1024.  The split-K partial tiles live in a fixed 16 MiB
+ * `static __device__` array that every GPU loading this library holds until
+ * exit.  The first call on a device looks the array up (cudaGetSymbolAddress):
+ * make it before any stream capture.  Calls share the array, so calls whose
+ * kernels overlap on the GPU race; serialise them. */
+DT_API int dt_gram_f64_noalloc(dt_ctx *ctx, const double *X, int ndim, const int64_t *shape,
+                               int mode, double *G);
+
 /* C = A_(mode) B_(mode)^T, shapeA[mode] x shapeB[mode] col-major; the other
  * modes of A and B must agree.  Replaces Function::ttt_except (tensor.tpp:132-259). */
 DT_API int dt_ttt_except_f64(dt_ctx *ctx, const double *A, const int64_t *shapeA, const double *B,
