@@ -371,6 +371,334 @@ __global__ void __launch_bounds__(LA_NT) subspace_kernel(const double *Sg, int64
     for (int64_t e = t; e < n * r; e += blockDim.x) Lg[e] = cur_in[e];
 }
 
+// ---------------------------------------------------------------------------
+// Register-tiled subspace iteration for n <= 256 and r <= RT (8, 16 or 32), one
+// CTA of 256 threads.  Same schedule and arithmetic as subspace_kernel (five
+// products, CholeskyQR after the 2nd and 4th, CholeskyQR2 after the 5th), laid
+// out for throughput instead of one output per thread:
+//  * Z and Q are row-major n x RT in smem with a row pitch of RT + 2 doubles
+//    (16-byte rows for double2 loads; rows i..i+7 land on distinct banks);
+//    the columns r..RT-1 are zero padding;
+//  * S Z and Z R^{-1}: thread (rs, cg) keeps MR rows x 4 columns of the output
+//    in registers, so each shared load feeds 4 FMAs;
+//  * the r x r Gram: 4 x 4 register blocks, rows split over PARTS threads and
+//    summed in a fixed order (G stays exactly symmetric);
+//  * Cholesky and R^{-1} in warp 0 with rsqrt per pivot and multiplications by
+//    the reciprocal diagonal (no divides on the dependency chain).
+// A Cholesky breakdown restarts from the caller's L with Householder steps.
+// ---------------------------------------------------------------------------
+constexpr int ST_NT = 256;
+constexpr int ST_GP = 2048;  // doubles of Gram partials
+
+template <int SMODE>
+__device__ __forceinline__ double st_s(const double *Ss, const double *__restrict__ Sg, int n,
+                                       int i, int k) {
+    if (SMODE == S_FULL) return Ss[i + n * k];
+    if (SMODE == S_PACKED) {
+        const int a = i < k ? i : k, b = i < k ? k : i;
+        return Ss[a + (b * (b + 1)) / 2];
+    }
+    return __ldg(Sg + i + (int64_t)n * k);
+}
+
+template <int RT>
+struct StTile {
+    static constexpr int LD = RT + 2;
+    static constexpr int CG = RT / 4;
+    static constexpr int RS = ST_NT / CG;
+    static constexpr int MR = 256 / RS;  // covers n <= 256
+};
+
+// dst(i, c) = sum_k s(i, k) src(k, c).
+template <int RT, int SMODE>
+__device__ __forceinline__ void st_product(const double *Ss, const double *Sg, int n,
+                                           const double *src, double *dst) {
+    using T = StTile<RT>;
+    const int t = threadIdx.x, cg = t % T::CG, rs = t / T::CG;
+    double acc[T::MR][4];
+#pragma unroll
+    for (int m = 0; m < T::MR; m++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) acc[m][v] = 0.0;
+#pragma unroll 2
+    for (int k = 0; k < n; k++) {
+        const double2 q01 = *reinterpret_cast<const double2 *>(src + k * T::LD + 4 * cg);
+        const double2 q23 = *reinterpret_cast<const double2 *>(src + k * T::LD + 4 * cg + 2);
+#pragma unroll
+        for (int m = 0; m < T::MR; m++) {
+            const int i = rs + T::RS * m;
+            if (i < n) {
+                const double sv = st_s<SMODE>(Ss, Sg, n, i, k);
+                acc[m][0] = fma(sv, q01.x, acc[m][0]);
+                acc[m][1] = fma(sv, q01.y, acc[m][1]);
+                acc[m][2] = fma(sv, q23.x, acc[m][2]);
+                acc[m][3] = fma(sv, q23.y, acc[m][3]);
+            }
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < T::MR; m++) {
+        const int i = rs + T::RS * m;
+        if (i < n) {
+            *reinterpret_cast<double2 *>(dst + i * T::LD + 4 * cg) = make_double2(acc[m][0], acc[m][1]);
+            *reinterpret_cast<double2 *>(dst + i * T::LD + 4 * cg + 2) =
+                make_double2(acc[m][2], acc[m][3]);
+        }
+    }
+}
+
+// dst(i, c) = sum_{j} src(i, j) Ri(j, c)   (Ri row-major RT x RT, upper).
+template <int RT>
+__device__ __forceinline__ void st_apply(const double *src, const double *Ri, int n, int r,
+                                         double *dst) {
+    using T = StTile<RT>;
+    const int t = threadIdx.x, cg = t % T::CG, rs = t / T::CG;
+    double acc[T::MR][4];
+#pragma unroll
+    for (int m = 0; m < T::MR; m++)
+#pragma unroll
+        for (int v = 0; v < 4; v++) acc[m][v] = 0.0;
+    for (int j = 0; j < r; j++) {
+        const double2 q01 = *reinterpret_cast<const double2 *>(Ri + j * RT + 4 * cg);
+        const double2 q23 = *reinterpret_cast<const double2 *>(Ri + j * RT + 4 * cg + 2);
+#pragma unroll
+        for (int m = 0; m < T::MR; m++) {
+            const int i = rs + T::RS * m;
+            if (i < n) {
+                const double z = src[i * T::LD + j];
+                acc[m][0] = fma(z, q01.x, acc[m][0]);
+                acc[m][1] = fma(z, q01.y, acc[m][1]);
+                acc[m][2] = fma(z, q23.x, acc[m][2]);
+                acc[m][3] = fma(z, q23.y, acc[m][3]);
+            }
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < T::MR; m++) {
+        const int i = rs + T::RS * m;
+        if (i < n) {
+            *reinterpret_cast<double2 *>(dst + i * T::LD + 4 * cg) = make_double2(acc[m][0], acc[m][1]);
+            *reinterpret_cast<double2 *>(dst + i * T::LD + 4 * cg + 2) =
+                make_double2(acc[m][2], acc[m][3]);
+        }
+    }
+}
+
+// G = src^T src (RT x RT row-major); rows/columns >= r replaced by the identity.
+template <int RT>
+__device__ __forceinline__ void st_gram(const double *src, int n, int r, double *Gp, double *G) {
+    using T = StTile<RT>;
+    constexpr int BG = RT / 4, NB = BG * BG;
+    constexpr int P1 = ST_NT / NB, P2 = ST_GP / (RT * RT);
+    constexpr int PARTS = P1 < P2 ? P1 : P2;
+    const int t = threadIdx.x;
+    if (t < NB * PARTS) {
+        const int blk = t % NB, part = t / NB, ab = blk % BG, bb = blk / BG;
+        double acc[4][4];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+            for (int v = 0; v < 4; v++) acc[u][v] = 0.0;
+        for (int i = part; i < n; i += PARTS) {
+            const double2 x01 = *reinterpret_cast<const double2 *>(src + i * T::LD + 4 * ab);
+            const double2 x23 = *reinterpret_cast<const double2 *>(src + i * T::LD + 4 * ab + 2);
+            const double2 y01 = *reinterpret_cast<const double2 *>(src + i * T::LD + 4 * bb);
+            const double2 y23 = *reinterpret_cast<const double2 *>(src + i * T::LD + 4 * bb + 2);
+            const double a[4] = {x01.x, x01.y, x23.x, x23.y};
+            const double b[4] = {y01.x, y01.y, y23.x, y23.y};
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int v = 0; v < 4; v++) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+#pragma unroll
+            for (int v = 0; v < 4; v++)
+                Gp[part * RT * RT + (4 * ab + u) * RT + 4 * bb + v] = acc[u][v];
+    }
+    __syncthreads();
+    for (int e = t; e < RT * RT; e += ST_NT) {
+        double s = 0.0;
+#pragma unroll
+        for (int p = 0; p < PARTS; p++) s += Gp[p * RT * RT + e];
+        const int a = e / RT, b = e % RT;
+        if (a >= r || b >= r) s = (a == b) ? 1.0 : 0.0;
+        G[e] = s;
+    }
+    __syncthreads();
+}
+
+// Warp 0: G = R^T R (R upper), Ri = R^{-1}, both row-major RT x RT.  Lane c
+// holds column c of G / R during the factorisation; R (overwriting G) and the
+// reciprocal diagonal (dinv) then go through shared memory, so the inverse
+// keeps only its own column in registers.  Returns false on a non-positive pivot.
+template <int RT>
+__device__ __forceinline__ bool st_chol_inv(double *G, double *Ri, double *dinv, int r) {
+    const int lane = threadIdx.x & 31;
+    const bool act = lane < RT;
+    bool ok;
+    {
+        double g[RT];
+#pragma unroll
+        for (int i = 0; i < RT; i++) g[i] = act ? G[i * RT + lane] : 0.0;
+        const double g00 = __shfl_sync(0xffffffffu, g[0], 0);
+        ok = g00 > 0.0;
+#pragma unroll
+        for (int k = 0; k < RT; k++) {
+            if (k < r) {
+                const double d = __shfl_sync(0xffffffffu, g[k], k);
+                ok = ok && (d > 1e-28 * g00);
+                const double ri = rsqrt(fmax(d, 1e-300));
+                if (lane == k) dinv[k] = ri;
+                if (lane >= k) g[k] *= ri;
+#pragma unroll
+                for (int i = k + 1; i < RT; i++) {
+                    if (i < r) {
+                        const double rki = __shfl_sync(0xffffffffu, g[k], i);
+                        if (lane >= i) g[i] = fma(-rki, g[k], g[i]);
+                    }
+                }
+            } else if (lane == k) {
+                dinv[k] = 1.0;
+            }
+        }
+        if (act) {
+#pragma unroll
+            for (int i = 0; i < RT; i++) G[i * RT + lane] = i <= lane ? g[i] : 0.0;
+        }
+    }
+    __syncwarp();
+    // Column `lane` of R^{-1}: x_i = (delta_{i,lane} - sum_{j>i} R(i,j) x_j) / R(i,i).
+    double x[RT];
+#pragma unroll
+    for (int i = RT - 1; i >= 0; i--) {
+        double s0 = (i == lane) ? 1.0 : 0.0, s1 = 0.0;
+#pragma unroll
+        for (int j = i + 1; j < RT; j++) {
+            const double rij = G[i * RT + j];
+            if (j & 1)
+                s1 = fma(-rij, x[j], s1);
+            else
+                s0 = fma(-rij, x[j], s0);
+        }
+        x[i] = (s0 + s1) * dinv[i];
+    }
+    if (act) {
+#pragma unroll
+        for (int i = 0; i < RT; i++) Ri[i * RT + lane] = i <= lane ? x[i] : 0.0;
+    }
+    __syncwarp();
+    return ok;
+}
+
+template <int RT, int SMODE>
+__global__ void __launch_bounds__(ST_NT) subspace_tile_kernel(const double *Sg, int n,
+                                                              double *Lg, int r, int iters,
+                                                              double *work, int *flag) {
+    using T = StTile<RT>;
+    extern __shared__ __align__(16) double sm[];
+    __shared__ double red[33];
+    __shared__ int bad;
+    const int t = threadIdx.x;
+    double *A = sm;
+    double *B = A + n * T::LD;
+    double *Gp = B + n * T::LD;
+    double *G = Gp + ST_GP;
+    double *Ri = G + RT * RT;
+    double *Ss = Ri + RT * RT;
+    if (SMODE == S_FULL) {
+        for (int e = t; e < n * n; e += ST_NT) Ss[e] = Sg[e];
+    } else if (SMODE == S_PACKED) {
+        for (int e = t; e < n * n; e += ST_NT) {
+            const int i = e % n, k = e / n;
+            if (i <= k) Ss[i + (k * (k + 1)) / 2] = Sg[e];
+        }
+    }
+    for (int e = t; e < n * RT; e += ST_NT) {
+        const int i = e / RT, c = e % RT;
+        A[i * T::LD + c] = c < r ? Lg[i + (int64_t)n * c] : 0.0;
+    }
+    if (t == 0) bad = 0;
+    __syncthreads();
+
+    double *cur = A, *oth = B;
+    for (int it = 0; it < iters; it++) {
+        st_product<RT, SMODE>(Ss, Sg, n, cur, oth);
+        __syncthreads();
+        double *tmp = cur;
+        cur = oth;
+        oth = tmp;
+        const bool last = it == iters - 1;
+        if (last || (it & 1)) {
+            const int passes = last ? 2 : 1;
+            for (int p = 0; p < passes; p++) {
+                st_gram<RT>(cur, n, r, Gp, G);
+                if (t < 32) {
+                    const bool ok = st_chol_inv<RT>(G, Ri, Gp, r);
+                    if (t == 0 && !ok) bad = 1;
+                }
+                __syncthreads();
+                if (bad) break;
+                st_apply<RT>(cur, Ri, n, r, oth);
+                __syncthreads();
+                tmp = cur;
+                cur = oth;
+                oth = tmp;
+            }
+            if (bad) break;
+        }
+    }
+    if (!bad) {
+        for (int e = t; e < n * r; e += ST_NT) {
+            const int i = e % n, c = e / n;
+            Lg[e] = cur[i * T::LD + c];
+        }
+        return;
+    }
+    // Rank-deficient or badly conditioned: restart from the caller's L and run
+    // every step with Householder orthonormalisation (col-major, in `work`).
+    double *Lw = work, *hw = work + 2 * (int64_t)n * r;
+    for (int e = t; e < n * r; e += ST_NT) Lw[e] = Lg[e];
+    __syncthreads();
+    for (int it = 0; it < iters; it++) {
+        for (int e = t; e < n * r; e += ST_NT) {
+            const int i = e % n, c = e / n;
+            double acc = 0.0;
+            for (int k = 0; k < n; k++) acc = fma(st_s<SMODE>(Ss, Sg, n, i, k), Lw[k + n * c], acc);
+            hw[e] = acc;
+        }
+        __syncthreads();
+        hqr_device(hw, n, r, hw + (int64_t)n * r, Lw, red);
+        __syncthreads();
+    }
+    if (t == 0 && flag) atomicOr(flag, 2);
+    for (int e = t; e < n * r; e += ST_NT) Lg[e] = Lw[e];
+}
+
+template <int RT, int SMODE>
+void launch_subspace_tile(dt_ctx *ctx, const double *S, int n, double *L, int r, int iters,
+                          double *work, int *flag, size_t smem) {
+    auto kern = subspace_tile_kernel<RT, SMODE>;
+    DT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    DT_LAUNCH(ctx, kern, 1, ST_NT, smem, S, n, L, r, iters, work, flag);
+}
+
+template <int RT>
+void subspace_tile(dt_ctx *ctx, const double *S, int n, double *L, int r, int iters,
+                   double *work, int *flag) {
+    const size_t base = (2 * (size_t)n * StTile<RT>::LD + ST_GP + 2 * RT * RT) * sizeof(double);
+    const size_t full = (size_t)n * n * sizeof(double);
+    const size_t packed = (size_t)n * (n + 1) / 2 * sizeof(double);
+    const size_t cap = 220 * 1024;
+    if (base + full <= cap)
+        launch_subspace_tile<RT, S_FULL>(ctx, S, n, L, r, iters, work, flag, base + full);
+    else if (base + packed <= cap)
+        launch_subspace_tile<RT, S_PACKED>(ctx, S, n, L, r, iters, work, flag, base + packed);
+    else
+        launch_subspace_tile<RT, S_GLOBAL>(ctx, S, n, L, r, iters, work, flag, base);
+}
+
 // Subspace iteration for ranks above 32: Householder QR every step, S, L and Z
 // in global memory (L2-resident).  work >= 3*n*r + r.
 __global__ void __launch_bounds__(LA_NT) subspace_wide_kernel(const double *S, int64_t n,
@@ -623,6 +951,15 @@ void subspace_iter(dt_ctx *ctx, const double *S, int64_t n, double *L, int64_t r
                  (long long)r);
     if (r > 32) {
         DT_LAUNCH(ctx, subspace_wide_kernel, 1, LA_NT, 0, S, n, L, r, iters, work);
+        return;
+    }
+    if (n <= 256) {
+        if (r <= 8)
+            subspace_tile<8>(ctx, S, (int)n, L, (int)r, iters, work, flag);
+        else if (r <= 16)
+            subspace_tile<16>(ctx, S, (int)n, L, (int)r, iters, work, flag);
+        else
+            subspace_tile<32>(ctx, S, (int)n, L, (int)r, iters, work, flag);
         return;
     }
     const size_t base = 2 * r * r * sizeof(double);

@@ -116,6 +116,20 @@ def test_als_vs_reference(ctx, oracle_ref):
     np.testing.assert_allclose(q.T @ q, np.eye(4), atol=1e-13)
 
 
+@pytest.mark.parametrize("n,r", [(96, 16), (97, 13), (150, 16), (200, 10), (256, 8), (64, 32),
+                                 (40, 20), (5, 5), (33, 1), (300, 12)])
+def test_als_subspace_sizes_vs_oracle(ctx, n, r):
+    """dt_als_f64 over the subspace kernel's shapes: S staged whole, packed, or
+    read from L2; ranks padded to 8, 16 and 32; n above the tiled kernel's 256."""
+    rng = np.random.default_rng(n * 100 + r)
+    Y = np.asfortranarray(rng.standard_normal((n, 12, max(4, (2 * n) // 12 + 1))))
+    L0, _ = np.linalg.qr(rng.standard_normal((n, r)))
+    q = ctx.als(Y, 0, L0, 5)
+    want = dense.als(Y, 0, L0, 5)
+    assert dense.principal_angle_max(q, want) < 1e-10
+    np.testing.assert_allclose(q.T @ q, np.eye(r), atol=1e-13)
+
+
 def _check_hooi(G, U, rep, gn_ref, U_ref, xn):
     assert abs(rep["g_norm"] - gn_ref) <= 1e-10 * gn_ref
     assert abs(np.linalg.norm(G) - gn_ref) <= 1e-10 * gn_ref
