@@ -9,11 +9,18 @@
 #include <cstdio>
 #include <stdexcept>
 #include <string>
+#include <unordered_set>
 #include <vector>
 
 #include "dt_cuda.h"
 
+struct dt_sptensor;
+
 struct dt_ctx {
+    // Sparse tensors created on this context; dt_ctx_destroy frees their device
+    // memory and detaches them, so a later dt_sptensor_destroy only frees the
+    // host object.
+    std::unordered_set<dt_sptensor *> sptensors;
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
@@ -86,6 +93,10 @@ inline void check_ctx(const dt_ctx *ctx) {
 }
 
 bool is_device_ptr(const void *p);
+
+// Frees the device memory of every sparse tensor still attached to ctx and
+// detaches it (called by dt_ctx_destroy).
+void detach_sptensors(dt_ctx *ctx);
 
 // Stream-ordered device allocation owned by one call.
 class DevMem {

@@ -109,6 +109,7 @@ int dt_ctx_destroy(dt_ctx *ctx) {
     return guard([&] {
         if (!ctx) return;
         cudaSetDevice(ctx->device);
+        detach_sptensors(ctx);
         if (ctx->stream) cudaStreamSynchronize(ctx->stream);
         if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
         if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);

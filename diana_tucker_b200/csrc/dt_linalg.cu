@@ -372,200 +372,203 @@ __global__ void __launch_bounds__(LA_NT) subspace_kernel(const double *Sg, int64
 }
 
 // ---------------------------------------------------------------------------
-// Register-tiled subspace iteration for n <= 256 and r <= RT (8, 16 or 32), one
-// CTA of 256 threads.  Same schedule and arithmetic as subspace_kernel (five
-// products, CholeskyQR after the 2nd and 4th, CholeskyQR2 after the 5th), laid
-// out for throughput instead of one output per thread:
-//  * Z and Q are row-major n x RT in smem with a row pitch of RT + 2 doubles
-//    (16-byte rows for double2 loads; rows i..i+7 land on distinct banks);
-//    the columns r..RT-1 are zero padding;
-//  * S Z and Z R^{-1}: thread (rs, cg) keeps MR rows x 4 columns of the output
-//    in registers, so each shared load feeds 4 FMAs;
-//  * the r x r Gram: 4 x 4 register blocks, rows split over PARTS threads and
-//    summed in a fixed order (G stays exactly symmetric);
-//  * Cholesky and R^{-1} in warp 0 with rsqrt per pivot and multiplications by
-//    the reciprocal diagonal (no divides on the dependency chain).
-// A Cholesky breakdown restarts from the caller's L with Householder steps.
+// Subspace iteration on the FP64 tensor-core path (mma.sync m8n8k4 .f64) for
+// n <= 256 and r <= RT (8, 16 or 32), one CTA of 8 warps.  Same schedule as
+// subspace_kernel (five products S Z, CholeskyQR after the 2nd and 4th,
+// CholeskyQR2 after the 5th).  Shared-memory layout:
+//  * S col-major with a leading dimension LDS = 4 (mod 16) and Z, Q row-major
+//    n8 x RT with pitch RT + 4: the 8 x 4 and 4 x 8 operand fragments then hit
+//    16 distinct 8-byte bank pairs per half-warp;
+//  * rows n..n8-1 and columns r..RT-1 are zero padding, so every product,
+//    Gram and solve runs on whole 8 x 8 tiles.
+// S Z and Z R^{-1}: each warp owns whole m-tile rows (all RT/8 n-tiles, two
+// m-tiles interleaved).  Z^T Z: whole K split over warps when it has fewer
+// than 8 tiles, partials summed in a fixed order.  Cholesky and R^{-1} in
+// warp 0 (rsqrt per pivot, multiplications by the reciprocal diagonal).  A
+// Cholesky breakdown restarts from the caller's L with Householder steps.
 // ---------------------------------------------------------------------------
-constexpr int ST_NT = 256;
-constexpr int ST_GP = 2048;  // doubles of Gram partials
+constexpr int SM_WARPS = 8;
+constexpr int SM_NT = SM_WARPS * 32;
+constexpr int SM_GP = 512;  // doubles of Gram partials (K split only below 8 tiles)
 
-template <int SMODE>
-__device__ __forceinline__ double st_s(const double *Ss, const double *__restrict__ Sg, int n,
-                                       int i, int k) {
-    if (SMODE == S_FULL) return Ss[i + n * k];
-    if (SMODE == S_PACKED) {
-        const int a = i < k ? i : k, b = i < k ? k : i;
-        return Ss[a + (b * (b + 1)) / 2];
-    }
-    return __ldg(Sg + i + (int64_t)n * k);
+__device__ __forceinline__ void dmma884(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
 }
 
 template <int RT>
-struct StTile {
-    static constexpr int LD = RT + 2;
-    static constexpr int CG = RT / 4;
-    static constexpr int RS = ST_NT / CG;
-    static constexpr int MR = 256 / RS;  // covers n <= 256
+struct SmTile {
+    static constexpr int LDQ = RT + 4;  // Z / Q pitch (= 4 mod 16 for RT in {16, 32}; 12 for 8)
+    static constexpr int LDR = RT + 4;  // R^{-1} pitch
+    static constexpr int NT = RT / 8;   // n-tiles
 };
 
-// dst(i, c) = sum_k s(i, k) src(k, c).
+__host__ __device__ inline int sm_lds(int n8) { return ((n8 + 11) / 16) * 16 + 4; }
+
+// dst = S src   (n8 x RT), S from shared (ld lds) or from global (ld n).
 template <int RT, int SMODE>
-__device__ __forceinline__ void st_product(const double *Ss, const double *Sg, int n,
-                                           const double *src, double *dst) {
-    using T = StTile<RT>;
-    const int t = threadIdx.x, cg = t % T::CG, rs = t / T::CG;
-    double acc[T::MR][4];
+__device__ __forceinline__ void sm_product(const double *Ss, int lds, const double *__restrict__ Sg,
+                                           int n, int n8, const double *src, double *dst) {
+    using T = SmTile<RT>;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int mtiles = n8 / 8, ksteps = (n + 3) / 4;
+    for (int mt0 = w; mt0 < mtiles; mt0 += 2 * SM_WARPS) {
+        const int mt1 = mt0 + SM_WARPS;
+        const bool two = mt1 < mtiles;
+        double acc[2][T::NT][2];
 #pragma unroll
-    for (int m = 0; m < T::MR; m++)
+        for (int m = 0; m < 2; m++)
 #pragma unroll
-        for (int v = 0; v < 4; v++) acc[m][v] = 0.0;
-#pragma unroll 2
-    for (int k = 0; k < n; k++) {
-        const double2 q01 = *reinterpret_cast<const double2 *>(src + k * T::LD + 4 * cg);
-        const double2 q23 = *reinterpret_cast<const double2 *>(src + k * T::LD + 4 * cg + 2);
+            for (int j = 0; j < T::NT; j++) acc[m][j][0] = acc[m][j][1] = 0.0;
+        const int i0 = 8 * mt0 + g, i1 = 8 * mt1 + g;
+#pragma unroll 4
+        for (int kk = 0; kk < ksteps; kk++) {
+            const int k = 4 * kk + t;
+            double a0, a1 = 0.0;
+            if (SMODE == S_FULL) {
+                a0 = Ss[i0 + lds * k];
+                if (two) a1 = Ss[i1 + lds * k];
+            } else {
+                a0 = (i0 < n && k < n) ? __ldg(Sg + i0 + (int64_t)n * k) : 0.0;
+                if (two) a1 = (i1 < n && k < n) ? __ldg(Sg + i1 + (int64_t)n * k) : 0.0;
+            }
 #pragma unroll
-        for (int m = 0; m < T::MR; m++) {
-            const int i = rs + T::RS * m;
-            if (i < n) {
-                const double sv = st_s<SMODE>(Ss, Sg, n, i, k);
-                acc[m][0] = fma(sv, q01.x, acc[m][0]);
-                acc[m][1] = fma(sv, q01.y, acc[m][1]);
-                acc[m][2] = fma(sv, q23.x, acc[m][2]);
-                acc[m][3] = fma(sv, q23.y, acc[m][3]);
+            for (int j = 0; j < T::NT; j++) {
+                const double b = src[k * T::LDQ + 8 * j + g];
+                dmma884(acc[0][j][0], acc[0][j][1], a0, b);
+                if (two) dmma884(acc[1][j][0], acc[1][j][1], a1, b);
             }
         }
-    }
 #pragma unroll
-    for (int m = 0; m < T::MR; m++) {
-        const int i = rs + T::RS * m;
-        if (i < n) {
-            *reinterpret_cast<double2 *>(dst + i * T::LD + 4 * cg) = make_double2(acc[m][0], acc[m][1]);
-            *reinterpret_cast<double2 *>(dst + i * T::LD + 4 * cg + 2) =
-                make_double2(acc[m][2], acc[m][3]);
+        for (int m = 0; m < 2; m++) {
+            if (m == 1 && !two) break;
+            const int row = 8 * (m ? mt1 : mt0) + g;
+#pragma unroll
+            for (int j = 0; j < T::NT; j++)
+                *reinterpret_cast<double2 *>(dst + row * T::LDQ + 8 * j + 2 * t) =
+                    make_double2(acc[m][j][0], acc[m][j][1]);
         }
     }
 }
 
-// dst(i, c) = sum_{j} src(i, j) Ri(j, c)   (Ri row-major RT x RT, upper).
+// dst = src Ri   (n8 x RT times RT x RT upper).
 template <int RT>
-__device__ __forceinline__ void st_apply(const double *src, const double *Ri, int n, int r,
+__device__ __forceinline__ void sm_apply(const double *src, const double *Ri, int n8,
                                          double *dst) {
-    using T = StTile<RT>;
-    const int t = threadIdx.x, cg = t % T::CG, rs = t / T::CG;
-    double acc[T::MR][4];
+    using T = SmTile<RT>;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int mtiles = n8 / 8;
+    for (int mt = w; mt < mtiles; mt += SM_WARPS) {
+        double acc[T::NT][2];
 #pragma unroll
-    for (int m = 0; m < T::MR; m++)
+        for (int j = 0; j < T::NT; j++) acc[j][0] = acc[j][1] = 0.0;
+        const int row = 8 * mt + g;
 #pragma unroll
-        for (int v = 0; v < 4; v++) acc[m][v] = 0.0;
-    for (int j = 0; j < r; j++) {
-        const double2 q01 = *reinterpret_cast<const double2 *>(Ri + j * RT + 4 * cg);
-        const double2 q23 = *reinterpret_cast<const double2 *>(Ri + j * RT + 4 * cg + 2);
+        for (int kk = 0; kk < RT / 4; kk++) {
+            const double a = src[row * T::LDQ + 4 * kk + t];
 #pragma unroll
-        for (int m = 0; m < T::MR; m++) {
-            const int i = rs + T::RS * m;
-            if (i < n) {
-                const double z = src[i * T::LD + j];
-                acc[m][0] = fma(z, q01.x, acc[m][0]);
-                acc[m][1] = fma(z, q01.y, acc[m][1]);
-                acc[m][2] = fma(z, q23.x, acc[m][2]);
-                acc[m][3] = fma(z, q23.y, acc[m][3]);
-            }
+            for (int j = 0; j < T::NT; j++)
+                dmma884(acc[j][0], acc[j][1], a, Ri[(4 * kk + t) * T::LDR + 8 * j + g]);
         }
-    }
 #pragma unroll
-    for (int m = 0; m < T::MR; m++) {
-        const int i = rs + T::RS * m;
-        if (i < n) {
-            *reinterpret_cast<double2 *>(dst + i * T::LD + 4 * cg) = make_double2(acc[m][0], acc[m][1]);
-            *reinterpret_cast<double2 *>(dst + i * T::LD + 4 * cg + 2) =
-                make_double2(acc[m][2], acc[m][3]);
-        }
+        for (int j = 0; j < T::NT; j++)
+            *reinterpret_cast<double2 *>(dst + row * T::LDQ + 8 * j + 2 * t) =
+                make_double2(acc[j][0], acc[j][1]);
     }
 }
 
 // G = src^T src (RT x RT row-major); rows/columns >= r replaced by the identity.
 template <int RT>
-__device__ __forceinline__ void st_gram(const double *src, int n, int r, double *Gp, double *G) {
-    using T = StTile<RT>;
-    constexpr int BG = RT / 4, NB = BG * BG;
-    constexpr int P1 = ST_NT / NB, P2 = ST_GP / (RT * RT);
-    constexpr int PARTS = P1 < P2 ? P1 : P2;
-    const int t = threadIdx.x;
-    if (t < NB * PARTS) {
-        const int blk = t % NB, part = t / NB, ab = blk % BG, bb = blk / BG;
-        double acc[4][4];
-#pragma unroll
-        for (int u = 0; u < 4; u++)
-#pragma unroll
-            for (int v = 0; v < 4; v++) acc[u][v] = 0.0;
-        for (int i = part; i < n; i += PARTS) {
-            const double2 x01 = *reinterpret_cast<const double2 *>(src + i * T::LD + 4 * ab);
-            const double2 x23 = *reinterpret_cast<const double2 *>(src + i * T::LD + 4 * ab + 2);
-            const double2 y01 = *reinterpret_cast<const double2 *>(src + i * T::LD + 4 * bb);
-            const double2 y23 = *reinterpret_cast<const double2 *>(src + i * T::LD + 4 * bb + 2);
-            const double a[4] = {x01.x, x01.y, x23.x, x23.y};
-            const double b[4] = {y01.x, y01.y, y23.x, y23.y};
-#pragma unroll
-            for (int u = 0; u < 4; u++)
-#pragma unroll
-                for (int v = 0; v < 4; v++) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+__device__ __forceinline__ void sm_gram(const double *src, int n, int r, double *Gp, double *G) {
+    using T = SmTile<RT>;
+    constexpr int TILES = T::NT * T::NT;
+    constexpr int KSP = TILES >= SM_WARPS ? 1 : SM_WARPS / TILES;
+    static_assert(KSP == 1 || KSP * RT * RT <= SM_GP, "Gram partials");
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int ksteps = (n + 3) / 4;
+    if (KSP == 1) {
+        for (int tt = w; tt < TILES; tt += SM_WARPS) {
+            const int ta = tt % T::NT, tb = tt / T::NT;
+            double d0 = 0.0, d1 = 0.0;
+            for (int kk = 0; kk < ksteps; kk++) {
+                const int k = 4 * kk + t;
+                dmma884(d0, d1, src[k * T::LDQ + 8 * ta + g], src[k * T::LDQ + 8 * tb + g]);
+            }
+            const int a = 8 * ta + g, b = 8 * tb + 2 * t;
+            G[a * RT + b] = d0;
+            G[a * RT + b + 1] = d1;
         }
+        __syncthreads();
+    } else {
+        const int tt = w % TILES, part = w / TILES;
+        const int ta = tt % T::NT, tb = tt / T::NT;
+        double d0 = 0.0, d1 = 0.0;
+        for (int kk = part; kk < ksteps; kk += KSP) {
+            const int k = 4 * kk + t;
+            dmma884(d0, d1, src[k * T::LDQ + 8 * ta + g], src[k * T::LDQ + 8 * tb + g]);
+        }
+        const int a = 8 * ta + g, b = 8 * tb + 2 * t;
+        Gp[part * RT * RT + a * RT + b] = d0;
+        Gp[part * RT * RT + a * RT + b + 1] = d1;
+        __syncthreads();
+        for (int e = threadIdx.x; e < RT * RT; e += SM_NT) {
+            double s = 0.0;
 #pragma unroll
-        for (int u = 0; u < 4; u++)
-#pragma unroll
-            for (int v = 0; v < 4; v++)
-                Gp[part * RT * RT + (4 * ab + u) * RT + 4 * bb + v] = acc[u][v];
+            for (int p = 0; p < KSP; p++) s += Gp[p * RT * RT + e];
+            G[e] = s;
+        }
+        __syncthreads();
     }
-    __syncthreads();
-    for (int e = t; e < RT * RT; e += ST_NT) {
-        double s = 0.0;
-#pragma unroll
-        for (int p = 0; p < PARTS; p++) s += Gp[p * RT * RT + e];
+    for (int e = threadIdx.x; e < RT * RT; e += SM_NT) {
         const int a = e / RT, b = e % RT;
-        if (a >= r || b >= r) s = (a == b) ? 1.0 : 0.0;
-        G[e] = s;
+        if (a >= r || b >= r) G[e] = (a == b) ? 1.0 : 0.0;
     }
     __syncthreads();
 }
 
-// Warp 0: G = R^T R (R upper), Ri = R^{-1}, both row-major RT x RT.  Lane c
+// Warp 0: G = R^T R (R upper), Ri = R^{-1} (row-major, pitch LDR).  Lane c
 // holds column c of G / R during the factorisation; R (overwriting G) and the
 // reciprocal diagonal (dinv) then go through shared memory, so the inverse
 // keeps only its own column in registers.  Returns false on a non-positive pivot.
 template <int RT>
-__device__ __forceinline__ bool st_chol_inv(double *G, double *Ri, double *dinv, int r) {
+__device__ __forceinline__ bool sm_chol_inv(double *G, double *Ri, double *dinv, int r) {
+    constexpr int LDR = SmTile<RT>::LDR;
     const int lane = threadIdx.x & 31;
     const bool act = lane < RT;
     bool ok;
     {
-        double g[RT];
+        double gc[RT];
 #pragma unroll
-        for (int i = 0; i < RT; i++) g[i] = act ? G[i * RT + lane] : 0.0;
-        const double g00 = __shfl_sync(0xffffffffu, g[0], 0);
+        for (int i = 0; i < RT; i++) gc[i] = act ? G[i * RT + lane] : 0.0;
+        const double g00 = __shfl_sync(0xffffffffu, gc[0], 0);
         ok = g00 > 0.0;
 #pragma unroll
         for (int k = 0; k < RT; k++) {
             if (k < r) {
-                const double d = __shfl_sync(0xffffffffu, g[k], k);
+                const double d = __shfl_sync(0xffffffffu, gc[k], k);
                 ok = ok && (d > 1e-28 * g00);
                 const double ri = rsqrt(fmax(d, 1e-300));
                 if (lane == k) dinv[k] = ri;
-                if (lane >= k) g[k] *= ri;
+                if (lane >= k) gc[k] *= ri;
 #pragma unroll
                 for (int i = k + 1; i < RT; i++) {
                     if (i < r) {
-                        const double rki = __shfl_sync(0xffffffffu, g[k], i);
-                        if (lane >= i) g[i] = fma(-rki, g[k], g[i]);
+                        const double rki = __shfl_sync(0xffffffffu, gc[k], i);
+                        if (lane >= i) gc[i] = fma(-rki, gc[k], gc[i]);
                     }
                 }
             } else if (lane == k) {
                 dinv[k] = 1.0;
             }
         }
+        __syncwarp();
         if (act) {
 #pragma unroll
-            for (int i = 0; i < RT; i++) G[i * RT + lane] = i <= lane ? g[i] : 0.0;
+            for (int i = 0; i < RT; i++) G[i * RT + lane] = i <= lane ? gc[i] : 0.0;
         }
     }
     __syncwarp();
@@ -586,45 +589,59 @@ __device__ __forceinline__ bool st_chol_inv(double *G, double *Ri, double *dinv,
     }
     if (act) {
 #pragma unroll
-        for (int i = 0; i < RT; i++) Ri[i * RT + lane] = i <= lane ? x[i] : 0.0;
+        for (int i = 0; i < RT; i++) Ri[i * LDR + lane] = i <= lane ? x[i] : 0.0;
     }
     __syncwarp();
     return ok;
 }
 
+template <int RT>
+__host__ __device__ inline size_t sm_smem_doubles(int n, bool s_in_smem) {
+    const int n8 = (n + 7) / 8 * 8;
+    size_t d = 2 * (size_t)n8 * SmTile<RT>::LDQ   // Z, Q
+               + (size_t)SM_GP                    // Gram partials
+               + (size_t)RT * RT                  // G / R
+               + (size_t)RT * SmTile<RT>::LDR     // R^{-1}
+               + 32;                              // dinv
+    if (s_in_smem) d += (size_t)sm_lds(n8) * n8;
+    return d;
+}
+
 template <int RT, int SMODE>
-__global__ void __launch_bounds__(ST_NT) subspace_tile_kernel(const double *Sg, int n,
-                                                              double *Lg, int r, int iters,
-                                                              double *work, int *flag) {
-    using T = StTile<RT>;
+__global__ void __launch_bounds__(SM_NT, 1) subspace_mma_kernel(const double *Sg, int n,
+                                                             double *Lg, int r, int iters,
+                                                             double *work, int *flag) {
+    using T = SmTile<RT>;
     extern __shared__ __align__(16) double sm[];
     __shared__ double red[33];
     __shared__ int bad;
     const int t = threadIdx.x;
+    const int n8 = (n + 7) / 8 * 8;
+    const int lds = sm_lds(n8);
     double *A = sm;
-    double *B = A + n * T::LD;
-    double *Gp = B + n * T::LD;
-    double *G = Gp + ST_GP;
+    double *B = A + n8 * T::LDQ;
+    double *Gp = B + n8 * T::LDQ;
+    double *G = Gp + SM_GP;
     double *Ri = G + RT * RT;
-    double *Ss = Ri + RT * RT;
+    double *dinv = Ri + RT * T::LDR;
+    double *Ss = dinv + 32;
     if (SMODE == S_FULL) {
-        for (int e = t; e < n * n; e += ST_NT) Ss[e] = Sg[e];
-    } else if (SMODE == S_PACKED) {
-        for (int e = t; e < n * n; e += ST_NT) {
-            const int i = e % n, k = e / n;
-            if (i <= k) Ss[i + (k * (k + 1)) / 2] = Sg[e];
+        for (int e = t; e < lds * n8; e += SM_NT) {
+            const int i = e % lds, k = e / lds;
+            Ss[e] = (i < n && k < n) ? Sg[i + n * k] : 0.0;
         }
     }
-    for (int e = t; e < n * RT; e += ST_NT) {
-        const int i = e / RT, c = e % RT;
-        A[i * T::LD + c] = c < r ? Lg[i + (int64_t)n * c] : 0.0;
+    for (int e = t; e < n8 * T::LDQ; e += SM_NT) {
+        const int i = e / T::LDQ, c = e % T::LDQ;
+        A[e] = (i < n && c < r) ? Lg[i + (int64_t)n * c] : 0.0;
+        B[e] = 0.0;
     }
     if (t == 0) bad = 0;
     __syncthreads();
 
     double *cur = A, *oth = B;
     for (int it = 0; it < iters; it++) {
-        st_product<RT, SMODE>(Ss, Sg, n, cur, oth);
+        sm_product<RT, SMODE>(Ss, lds, Sg, n, n8, cur, oth);
         __syncthreads();
         double *tmp = cur;
         cur = oth;
@@ -633,14 +650,14 @@ __global__ void __launch_bounds__(ST_NT) subspace_tile_kernel(const double *Sg, 
         if (last || (it & 1)) {
             const int passes = last ? 2 : 1;
             for (int p = 0; p < passes; p++) {
-                st_gram<RT>(cur, n, r, Gp, G);
+                sm_gram<RT>(cur, n, r, Gp, G);
                 if (t < 32) {
-                    const bool ok = st_chol_inv<RT>(G, Ri, Gp, r);
+                    const bool ok = sm_chol_inv<RT>(G, Ri, dinv, r);
                     if (t == 0 && !ok) bad = 1;
                 }
                 __syncthreads();
                 if (bad) break;
-                st_apply<RT>(cur, Ri, n, r, oth);
+                sm_apply<RT>(cur, Ri, n8, oth);
                 __syncthreads();
                 tmp = cur;
                 cur = oth;
@@ -650,22 +667,25 @@ __global__ void __launch_bounds__(ST_NT) subspace_tile_kernel(const double *Sg, 
         }
     }
     if (!bad) {
-        for (int e = t; e < n * r; e += ST_NT) {
+        for (int e = t; e < n * r; e += SM_NT) {
             const int i = e % n, c = e / n;
-            Lg[e] = cur[i * T::LD + c];
+            Lg[e] = cur[i * T::LDQ + c];
         }
         return;
     }
     // Rank-deficient or badly conditioned: restart from the caller's L and run
     // every step with Householder orthonormalisation (col-major, in `work`).
     double *Lw = work, *hw = work + 2 * (int64_t)n * r;
-    for (int e = t; e < n * r; e += ST_NT) Lw[e] = Lg[e];
+    for (int e = t; e < n * r; e += SM_NT) Lw[e] = Lg[e];
     __syncthreads();
     for (int it = 0; it < iters; it++) {
-        for (int e = t; e < n * r; e += ST_NT) {
+        for (int e = t; e < n * r; e += SM_NT) {
             const int i = e % n, c = e / n;
             double acc = 0.0;
-            for (int k = 0; k < n; k++) acc = fma(st_s<SMODE>(Ss, Sg, n, i, k), Lw[k + n * c], acc);
+            for (int k = 0; k < n; k++) {
+                const double sv = SMODE == S_FULL ? Ss[i + lds * k] : __ldg(Sg + i + (int64_t)n * k);
+                acc = fma(sv, Lw[k + n * c], acc);
+            }
             hw[e] = acc;
         }
         __syncthreads();
@@ -673,30 +693,25 @@ __global__ void __launch_bounds__(ST_NT) subspace_tile_kernel(const double *Sg, 
         __syncthreads();
     }
     if (t == 0 && flag) atomicOr(flag, 2);
-    for (int e = t; e < n * r; e += ST_NT) Lg[e] = Lw[e];
+    for (int e = t; e < n * r; e += SM_NT) Lg[e] = Lw[e];
 }
 
 template <int RT, int SMODE>
-void launch_subspace_tile(dt_ctx *ctx, const double *S, int n, double *L, int r, int iters,
-                          double *work, int *flag, size_t smem) {
-    auto kern = subspace_tile_kernel<RT, SMODE>;
+void launch_subspace_mma(dt_ctx *ctx, const double *S, int n, double *L, int r, int iters,
+                         double *work, int *flag) {
+    const size_t smem = sm_smem_doubles<RT>(n, SMODE == S_FULL) * sizeof(double);
+    auto kern = subspace_mma_kernel<RT, SMODE>;
     DT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    DT_LAUNCH(ctx, kern, 1, ST_NT, smem, S, n, L, r, iters, work, flag);
+    DT_LAUNCH(ctx, kern, 1, SM_NT, smem, S, n, L, r, iters, work, flag);
 }
 
 template <int RT>
-void subspace_tile(dt_ctx *ctx, const double *S, int n, double *L, int r, int iters,
-                   double *work, int *flag) {
-    const size_t base = (2 * (size_t)n * StTile<RT>::LD + ST_GP + 2 * RT * RT) * sizeof(double);
-    const size_t full = (size_t)n * n * sizeof(double);
-    const size_t packed = (size_t)n * (n + 1) / 2 * sizeof(double);
-    const size_t cap = 220 * 1024;
-    if (base + full <= cap)
-        launch_subspace_tile<RT, S_FULL>(ctx, S, n, L, r, iters, work, flag, base + full);
-    else if (base + packed <= cap)
-        launch_subspace_tile<RT, S_PACKED>(ctx, S, n, L, r, iters, work, flag, base + packed);
+void subspace_mma(dt_ctx *ctx, const double *S, int n, double *L, int r, int iters,
+                  double *work, int *flag) {
+    if (sm_smem_doubles<RT>(n, true) * sizeof(double) <= 220 * 1024)
+        launch_subspace_mma<RT, S_FULL>(ctx, S, n, L, r, iters, work, flag);
     else
-        launch_subspace_tile<RT, S_GLOBAL>(ctx, S, n, L, r, iters, work, flag, base);
+        launch_subspace_mma<RT, S_GLOBAL>(ctx, S, n, L, r, iters, work, flag);
 }
 
 // Subspace iteration for ranks above 32: Householder QR every step, S, L and Z
@@ -955,11 +970,11 @@ void subspace_iter(dt_ctx *ctx, const double *S, int64_t n, double *L, int64_t r
     }
     if (n <= 256) {
         if (r <= 8)
-            subspace_tile<8>(ctx, S, (int)n, L, (int)r, iters, work, flag);
+            subspace_mma<8>(ctx, S, (int)n, L, (int)r, iters, work, flag);
         else if (r <= 16)
-            subspace_tile<16>(ctx, S, (int)n, L, (int)r, iters, work, flag);
+            subspace_mma<16>(ctx, S, (int)n, L, (int)r, iters, work, flag);
         else
-            subspace_tile<32>(ctx, S, (int)n, L, (int)r, iters, work, flag);
+            subspace_mma<32>(ctx, S, (int)n, L, (int)r, iters, work, flag);
         return;
     }
     const size_t base = 2 * r * r * sizeof(double);

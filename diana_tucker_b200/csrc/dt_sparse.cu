@@ -24,6 +24,8 @@ namespace {
 
 constexpr int MAXD = 8;
 constexpr int64_t CHUNK = 512;
+constexpr int64_t TASK_PACK = 512;
+constexpr int64_t TASK_PIECE = 2048;
 
 struct ModeCopy {
     // Nonzeros sorted by this mode's index.
@@ -41,6 +43,17 @@ struct ModeCopy {
     DevMem multi_row;     // int32 [nmulti]: compact row
     DevMem multi_first;   // int32 [nmulti]: first partial slot
     DevMem multi_count;   // int32 [nmulti]
+    // Task list of the 3-way TTMc kernel: runs of whole consecutive rows with
+    // at most TASK_PACK nonzeros in all, and pieces of at most TASK_PIECE
+    // nonzeros of longer rows; sorted by size, largest first.
+    int64_t ntasks = 0;
+    DevMem task_beg;      // int64 [ntasks]
+    DevMem task_end;      // int64 [ntasks]
+    DevMem task_row;      // int32 [ntasks]: compact row of the first nonzero
+    DevMem task_slot;     // int32 [ntasks]: -1 = rows written directly, else partial slot
+    int64_t tslots = 0;
+    int64_t tmulti = 0;   // rows cut into several pieces
+    DevMem tmulti_row, tmulti_first, tmulti_count;
 };
 
 struct FactorSet {
@@ -181,6 +194,202 @@ __global__ void __launch_bounds__(256) ttmc_rows_kernel(
     }
 }
 
+// ---------------------------------------------------------------------------
+// 3-way TTMc over the task list (even ranks RA, RB of the two other modes; P =
+// RA * RB).  One warp per task.  Nonzeros go through in batches of 32:
+//  * lane j loads nonzero j's two indices and value (coalesced); the batch
+//    after next is already in registers, so these loads overlap compute;
+//  * the two factor rows of every nonzero (RA + RB doubles) are copied into a
+//    per-warp shared stage with 16-byte cp.async, double-buffered: batch b+1
+//    is in flight while batch b is consumed;
+//  * lane l owns BPL blocks of AW x BW Kronecker entries (p = pa + RA * pb);
+//    per nonzero it reads AW + BW staged values and v, then AW*BW FMAs;
+//  * a packed task walks whole rows: at each row boundary (from a register
+//    window of 32 rowptr entries) the warp writes its row and restarts.
+// Long rows arrive as pieces that write partial rows, summed in piece order by
+// combine_partials_kernel: the output is deterministic, without atomics.
+// ---------------------------------------------------------------------------
+constexpr int T3_WARPS = 4;
+
+__device__ __forceinline__ void sp_cp_async16(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void sp_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void sp_cp_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int RA, int RB, int AW, int BW>
+struct T3 {
+    static constexpr int P = RA * RB;
+    static constexpr int NBA = RA / AW, NBB = RB / BW, NBLK = NBA * NBB;
+    static constexpr int BPL = (NBLK + 31) / 32;
+    static constexpr int ROWW = RA + RB;  // staged doubles per nonzero
+    static constexpr int PPN = ROWW / 2;  // 16-byte pieces per nonzero
+    static constexpr int STAGE = 32 * ROWW;
+    static constexpr int WARP_SMEM = 2 * STAGE + 32;  // doubles per warp
+};
+
+template <int RA, int RB, int AW, int BW>
+__global__ void __launch_bounds__(T3_WARPS * 32) ttmc3_kernel(
+    const int32_t *__restrict__ ia_arr, const int32_t *__restrict__ ib_arr,
+    const double *__restrict__ val, const int64_t *__restrict__ rowptr, int64_t nrows,
+    const int64_t *__restrict__ task_beg, const int64_t *__restrict__ task_end,
+    const int32_t *__restrict__ task_row, const int32_t *__restrict__ task_slot, int64_t ntasks,
+    const double *__restrict__ Ua, const double *__restrict__ Ub, double *__restrict__ Yc,
+    double *__restrict__ Ypart) {
+    using C = T3<RA, RB, AW, BW>;
+    static_assert(RA % 2 == 0 && RB % 2 == 0 && RA % AW == 0 && RB % BW == 0, "tile shape");
+    static_assert(AW == 1 || AW == 2, "AW");
+    static_assert(BW == 2 || BW == 4, "BW");
+    extern __shared__ __align__(16) double t3_smem[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double *stage0 = t3_smem + (size_t)wib * C::WARP_SMEM;
+    double *vbuf = stage0 + 2 * C::STAGE;
+    const int64_t gw = (int64_t)blockIdx.x * T3_WARPS + wib;
+    const int64_t nw = (int64_t)gridDim.x * T3_WARPS;
+
+    // Lane-owned blocks.
+    int oa[C::BPL], ob[C::BPL];
+    bool own[C::BPL];
+#pragma unroll
+    for (int q = 0; q < C::BPL; q++) {
+        const int blk = lane + 32 * q;
+        own[q] = blk < C::NBLK;
+        oa[q] = own[q] ? AW * (blk % C::NBA) : 0;
+        ob[q] = own[q] ? BW * (blk / C::NBA) : 0;
+    }
+
+    for (int64_t t = gw; t < ntasks; t += nw) {
+        const int64_t beg = task_beg[t], end = task_end[t];
+        int64_t row = task_row[t];
+        const int32_t slot = task_slot[t];
+        const int nb = (int)((end - beg + 31) / 32);
+
+        // Row-boundary window: lane l holds rowptr[wbase + 1 + l].
+        int64_t wbase = row;
+        int64_t bnd_win = (wbase + 1 + lane <= nrows) ? rowptr[wbase + 1 + lane] : INT64_MAX;
+        int wi = 0;
+
+        auto load_idx = [&](int b, int &ia, int &ib, double &v) {
+            const int64_t e = beg + 32 * (int64_t)b + lane;
+            const bool ok = e < end;
+            ia = ok ? ia_arr[e] : 0;
+            ib = ok ? ib_arr[e] : 0;
+            v = ok ? val[e] : 0.0;
+        };
+        auto issue = [&](int b, int ia, int ib) {
+            double *st = stage0 + (b & 1) * C::STAGE;
+            const int64_t e0 = beg + 32 * (int64_t)b;
+            const int n_b = (int)(end - e0 < 32 ? end - e0 : 32);
+#pragma unroll
+            for (int s = 0; s < C::PPN; s++) {
+                const int g = lane + 32 * s;
+                const int jj = g / C::PPN, rem = g - jj * C::PPN;
+                const int ija = __shfl_sync(0xffffffffu, ia, jj);
+                const int ijb = __shfl_sync(0xffffffffu, ib, jj);
+                if (jj < n_b) {
+                    const double *src = rem < RA / 2 ? Ua + (int64_t)ija * RA + 2 * rem
+                                                     : Ub + (int64_t)ijb * RB + 2 * (rem - RA / 2);
+                    sp_cp_async16(st + jj * C::ROWW + 2 * rem, src);
+                }
+            }
+            sp_cp_commit();
+        };
+
+        double acc[C::BPL][AW][BW];
+#pragma unroll
+        for (int q = 0; q < C::BPL; q++)
+#pragma unroll
+            for (int u = 0; u < AW; u++)
+#pragma unroll
+                for (int w = 0; w < BW; w++) acc[q][u][w] = 0.0;
+
+        auto flush = [&](int64_t r) {
+            double *dst = slot < 0 ? Yc + r * C::P : Ypart + (int64_t)slot * C::P;
+#pragma unroll
+            for (int q = 0; q < C::BPL; q++) {
+                if (!own[q]) continue;
+#pragma unroll
+                for (int w = 0; w < BW; w++) {
+                    double *d = dst + oa[q] + RA * (ob[q] + w);
+                    if (AW == 2)
+                        *reinterpret_cast<double2 *>(d) = make_double2(acc[q][0][w], acc[q][AW - 1][w]);
+                    else
+                        d[0] = acc[q][0][w];
+#pragma unroll
+                    for (int u = 0; u < AW; u++) acc[q][u][w] = 0.0;
+                }
+            }
+        };
+
+        int a_ia, a_ib;
+        double a_v, cur_v, nxt_v = 0.0;
+        load_idx(0, a_ia, a_ib, a_v);
+        issue(0, a_ia, a_ib);
+        cur_v = a_v;
+        if (nb > 1) load_idx(1, a_ia, a_ib, a_v);
+        int64_t next_bnd = __shfl_sync(0xffffffffu, bnd_win, 0);
+
+        for (int b = 0; b < nb; b++) {
+            if (b + 1 < nb) {
+                issue(b + 1, a_ia, a_ib);
+                nxt_v = a_v;
+                if (b + 2 < nb) load_idx(b + 2, a_ia, a_ib, a_v);
+                sp_cp_wait<1>();
+            } else {
+                sp_cp_wait<0>();
+            }
+            vbuf[lane] = cur_v;
+            __syncwarp();
+            const double *st = stage0 + (b & 1) * C::STAGE;
+            const int64_t e0 = beg + 32 * (int64_t)b;
+            const int n_b = (int)(end - e0 < 32 ? end - e0 : 32);
+            for (int j = 0; j < n_b; j++) {
+                if (e0 + j == next_bnd) {
+                    flush(row);
+                    row++;
+                    if (++wi == 32) {
+                        wbase += 32;
+                        wi = 0;
+                        bnd_win = (wbase + 1 + lane <= nrows) ? rowptr[wbase + 1 + lane] : INT64_MAX;
+                    }
+                    next_bnd = __shfl_sync(0xffffffffu, bnd_win, wi);
+                }
+                const double v = vbuf[j];
+                const double *srow = st + j * C::ROWW;
+#pragma unroll
+                for (int q = 0; q < C::BPL; q++) {
+                    if (!own[q]) continue;
+                    double wa[AW], ub[BW];
+                    if (AW == 2) {
+                        const double2 x = *reinterpret_cast<const double2 *>(srow + oa[q]);
+                        wa[0] = v * x.x;
+                        wa[AW - 1] = v * x.y;
+                    } else {
+                        wa[0] = v * srow[oa[q]];
+                    }
+#pragma unroll
+                    for (int w = 0; w < BW; w += 2) {
+                        const double2 y = *reinterpret_cast<const double2 *>(srow + RA + ob[q] + w);
+                        ub[w] = y.x;
+                        ub[w + 1] = y.y;
+                    }
+#pragma unroll
+                    for (int u = 0; u < AW; u++)
+#pragma unroll
+                        for (int w = 0; w < BW; w++) acc[q][u][w] = fma(wa[u], ub[w], acc[q][u][w]);
+                }
+            }
+            cur_v = nxt_v;
+            __syncwarp();
+        }
+        flush(row);
+    }
+}
+
 // Yc[row] = sum of its partial rows, in chunk order (deterministic).
 __global__ void combine_partials_kernel(const double *__restrict__ Ypart,
                                         const int32_t *__restrict__ multi_row,
@@ -199,73 +408,135 @@ __global__ void combine_partials_kernel(const double *__restrict__ Ypart,
     }
 }
 
-// mTL: out[:, rows[k]] = (Yc[k, :] L)^T, L is P x Rn col-major (in smem).
-// One warp per compact row; empty rows of out are zeroed beforehand.
-__global__ void __launch_bounds__(256) mtl_kernel(const double *__restrict__ Yc,
-                                                  const int32_t *__restrict__ rows,
-                                                  int64_t nrows, int P, const double *__restrict__ L,
-                                                  int Rn, double *__restrict__ out) {
-    extern __shared__ double Ls[];
-    for (int e = threadIdx.x; e < P * Rn; e += blockDim.x) Ls[e] = L[e];
-    __syncthreads();
-    const int lane = threadIdx.x & 31;
+// ---------------------------------------------------------------------------
+// ttmc_mTL / ttmc_mTR on the FP64 tensor-core path (mma.sync m8n8k4 .f64).
+// Operand fragments: A[g][t] and B[t][g] with g = lane / 4, t = lane % 4;
+// the 8 x 8 result D[g][2t + {0, 1}].  Staged shared operands use a pitch of
+// 4 (mod 16) doubles so a half-warp's fragment loads hit distinct banks.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void sp_dmma(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// out[rows[k] * Rn + r] = sum_p Yc[k, p] L[p + P r].  One warp per 8 compact
+// rows; NTL = ceil(Rn / 8) output tiles.  L staged in shared memory (pitch
+// 8 NTL + 4) when LSM, else read through the read-only cache.
+template <int NTL, bool LSM>
+__global__ void __launch_bounds__(256) mtl_mma_kernel(const double *__restrict__ Yc,
+                                                      const int32_t *__restrict__ rows,
+                                                      int64_t nrows, int P,
+                                                      const double *__restrict__ L, int Rn,
+                                                      double *__restrict__ out) {
+    constexpr int LDL = 8 * NTL + 4;
+    extern __shared__ __align__(16) double Ls[];
+    const int P4 = (P + 3) & ~3;
+    if (LSM) {
+        for (int e = threadIdx.x; e < P4 * LDL; e += blockDim.x) {
+            const int p = e / LDL, r = e - p * LDL;
+            Ls[e] = (p < P && r < Rn) ? L[p + (int64_t)P * r] : 0.0;
+        }
+        __syncthreads();
+    }
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     const int64_t warp0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t k = warp0; k < nrows; k += nwarps) {
-        const double *y = Yc + k * P;
-        double mine = 0.0;  // lane r < Rn ends up holding output r
-        for (int r = 0; r < Rn; r++) {
-            double s = 0.0;
-            for (int p = lane; p < P; p += 32) s = fma(y[p], Ls[p + (int64_t)P * r], s);
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-            if (lane == (r & 31)) mine = s;
-            if ((r & 31) == 31 || r == Rn - 1) {
-                const int base = r & ~31;
-                if (lane <= (r & 31)) out[(int64_t)rows[k] * Rn + base + lane] = mine;
+    const int64_t mtiles = (nrows + 7) / 8;
+    const int ksteps = P4 / 4;
+    for (int64_t mt = warp0; mt < mtiles; mt += nwarps) {
+        const int64_t k = 8 * mt + g;
+        const bool okr = k < nrows;
+        const double *y = Yc + (okr ? k : 0) * (int64_t)P;
+        double acc[NTL][2];
+#pragma unroll
+        for (int j = 0; j < NTL; j++) acc[j][0] = acc[j][1] = 0.0;
+#pragma unroll 8
+        for (int kk = 0; kk < ksteps; kk++) {
+            const int p = 4 * kk + t;
+            const double a = (okr && p < P) ? y[p] : 0.0;
+#pragma unroll
+            for (int j = 0; j < NTL; j++) {
+                const int r = 8 * j + g;
+                const double b = LSM ? Ls[p * LDL + r]
+                                     : ((p < P && r < Rn) ? __ldg(L + p + (int64_t)P * r) : 0.0);
+                sp_dmma(acc[j][0], acc[j][1], a, b);
+            }
+        }
+        if (okr) {
+            double *o = out + (int64_t)rows[k] * Rn;
+#pragma unroll
+            for (int j = 0; j < NTL; j++) {
+                const int r = 8 * j + 2 * t;
+                if (r < Rn) o[r] = acc[j][0];
+                if (r + 1 < Rn) o[r + 1] = acc[j][1];
             }
         }
     }
 }
 
-// mTR partials: part[blk][p + P*r] = sum over this block's compact rows of
-// Yc[k, p] * U_n(rows[k], r).  Thread t owns entries p = t, t + blockDim, ...
-// and keeps the R_n (<= 32) sums of its entry in registers.
-__global__ void __launch_bounds__(256) mtr_partial_kernel(const double *__restrict__ Yc,
-                                                          const int32_t *__restrict__ rows,
-                                                          int64_t nrows, int P,
-                                                          const double *__restrict__ Un, int Rn,
-                                                          int64_t rows_per_block,
-                                                          double *__restrict__ part) {
-    extern __shared__ double us[];  // staged U_n rows: [batch][Rn]
-    constexpr int BATCH = 32;
+// mTR partials: part[blk][p + P r] = sum over the block's compact rows k of
+// Yc[k, p] U(rows[k], r) (U transposed: row i at U + i Rn).  The block's rows
+// go through in batches of 64 whose U rows are staged in shared memory; warp
+// w owns p-tiles w, w + 8, ... (up to 4 at a time).
+template <int NTL>
+__global__ void __launch_bounds__(256) mtr_mma_kernel(const double *__restrict__ Yc,
+                                                      const int32_t *__restrict__ rows,
+                                                      int64_t nrows, int P,
+                                                      const double *__restrict__ U, int Rn,
+                                                      int64_t rows_per_block,
+                                                      double *__restrict__ part) {
+    constexpr int LDU = 8 * NTL + 4, KB = 64, MG = 4;
+    __shared__ __align__(16) double Us[KB * LDU];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
     const int64_t k0 = blockIdx.x * rows_per_block;
     const int64_t k1 = min(nrows, k0 + rows_per_block);
-    for (int p0 = 0; p0 < P; p0 += blockDim.x) {
-        const int p = p0 + threadIdx.x;
-        double acc[32];
+    const int ptiles = (P + 7) / 8;
+    double *pb = part + (int64_t)blockIdx.x * P * Rn;
+    for (int mbase = 0; mbase < ptiles; mbase += 8 * MG) {
+        double acc[MG][NTL][2];
 #pragma unroll
-        for (int r = 0; r < 32; r++) acc[r] = 0.0;
-        for (int64_t kb = k0; kb < k1; kb += BATCH) {
-            const int nb = (int)(k1 - kb < BATCH ? k1 - kb : BATCH);
+        for (int m = 0; m < MG; m++)
+#pragma unroll
+            for (int j = 0; j < NTL; j++) acc[m][j][0] = acc[m][j][1] = 0.0;
+        for (int64_t kb = k0; kb < k1; kb += KB) {
             __syncthreads();
-            for (int e = threadIdx.x; e < nb * Rn; e += blockDim.x) {
-                const int b = e / Rn, r = e % Rn;
-                us[e] = Un[(int64_t)rows[kb + b] * Rn + r];
+            for (int e = threadIdx.x; e < KB * LDU; e += blockDim.x) {
+                const int b = e / LDU, c = e - b * LDU;
+                const int64_t k = kb + b;
+                Us[e] = (k < k1 && c < Rn) ? U[(int64_t)rows[k] * Rn + c] : 0.0;
             }
             __syncthreads();
-            if (p < P) {
-                for (int b = 0; b < nb; b++) {
-                    const double yv = Yc[(kb + b) * P + p];
+            const int kn = (int)min((int64_t)KB, k1 - kb);
+            const int ks_end = (kn + 3) / 4;
+            for (int ks = 0; ks < ks_end; ks++) {
+                const int bl = 4 * ks + t;
+                const int64_t k = kb + bl;
+                const bool okk = bl < kn;
+                double bv[NTL];
 #pragma unroll
-                    for (int r = 0; r < 32; r++)
-                        if (r < Rn) acc[r] = fma(yv, us[b * Rn + r], acc[r]);
+                for (int j = 0; j < NTL; j++) bv[j] = Us[bl * LDU + 8 * j + g];
+#pragma unroll
+                for (int m = 0; m < MG; m++) {
+                    const int mt = mbase + w + 8 * m;
+                    const int p = 8 * mt + g;
+                    const double a = (okk && mt < ptiles && p < P) ? Yc[k * P + p] : 0.0;
+#pragma unroll
+                    for (int j = 0; j < NTL; j++) sp_dmma(acc[m][j][0], acc[m][j][1], a, bv[j]);
                 }
             }
         }
-        if (p < P) {
 #pragma unroll
-            for (int r = 0; r < 32; r++)
-                if (r < Rn) part[(int64_t)blockIdx.x * P * Rn + p + (int64_t)P * r] = acc[r];
+        for (int m = 0; m < MG; m++) {
+            const int mt = mbase + w + 8 * m;
+            const int p = 8 * mt + g;
+            if (mt >= ptiles || p >= P) continue;
+#pragma unroll
+            for (int j = 0; j < NTL; j++) {
+                const int r = 8 * j + 2 * t;
+                if (r < Rn) pb[p + (int64_t)P * r] = acc[m][j][0];
+                if (r + 1 < Rn) pb[p + (int64_t)P * (r + 1)] = acc[m][j][1];
+            }
         }
     }
 }
@@ -367,6 +638,59 @@ void build_mode(dt_ctx *ctx, dt_sptensor *sp, int n, const std::vector<DevMem> &
     mc.nchunks = (int64_t)crow.size();
     mc.nslots = slots;
     mc.nmulti = (int64_t)mrow.size();
+    // Tasks of the 3-way kernel.
+    struct Task {
+        int64_t beg, end;
+        int32_t row, slot;
+    };
+    std::vector<Task> tasks;
+    std::vector<int32_t> tmrow, tmfirst, tmcount;
+    int64_t tslots = 0;
+    {
+        int64_t pack_beg = -1;
+        int32_t pack_row = 0;
+        auto close_pack = [&](int64_t e) {
+            if (pack_beg >= 0) tasks.push_back({pack_beg, e, pack_row, -1});
+            pack_beg = -1;
+        };
+        for (int64_t k = 0; k < mc.nrows; k++) {
+            const int64_t b = rowptr[k], c = rowptr[k + 1] - b;
+            if (c > TASK_PACK) {
+                close_pack(b);
+                const int64_t np = (c + TASK_PIECE - 1) / TASK_PIECE;
+                if (np > 1) {
+                    tmrow.push_back((int32_t)k);
+                    tmfirst.push_back((int32_t)tslots);
+                    tmcount.push_back((int32_t)np);
+                }
+                for (int64_t j = 0; j < np; j++)
+                    tasks.push_back({b + j * TASK_PIECE, std::min(b + c, b + (j + 1) * TASK_PIECE),
+                                     (int32_t)k, np > 1 ? (int32_t)(tslots + j) : -1});
+                if (np > 1) tslots += np;
+                continue;
+            }
+            if (pack_beg >= 0 && b + c - pack_beg > TASK_PACK) close_pack(b);
+            if (pack_beg < 0) {
+                pack_beg = b;
+                pack_row = (int32_t)k;
+            }
+        }
+        close_pack(nnz);
+        std::stable_sort(tasks.begin(), tasks.end(), [](const Task &a, const Task &b) {
+            return a.end - a.beg > b.end - b.beg;
+        });
+    }
+    mc.ntasks = (int64_t)tasks.size();
+    mc.tslots = tslots;
+    mc.tmulti = (int64_t)tmrow.size();
+    std::vector<int64_t> tbeg(tasks.size()), tend(tasks.size());
+    std::vector<int32_t> trow(tasks.size()), tslot(tasks.size());
+    for (size_t i = 0; i < tasks.size(); i++) {
+        tbeg[i] = tasks[i].beg;
+        tend[i] = tasks[i].end;
+        trow[i] = tasks[i].row;
+        tslot[i] = tasks[i].slot;
+    }
     auto up = [&](DevMem &dst, const void *src, size_t bytes) {
         dst.alloc(ctx, std::max<size_t>(bytes, 8));
         if (bytes)
@@ -380,6 +704,13 @@ void build_mode(dt_ctx *ctx, dt_sptensor *sp, int n, const std::vector<DevMem> &
     up(mc.multi_row, mrow.data(), mrow.size() * sizeof(int32_t));
     up(mc.multi_first, mfirst.data(), mfirst.size() * sizeof(int32_t));
     up(mc.multi_count, mcount.data(), mcount.size() * sizeof(int32_t));
+    up(mc.task_beg, tbeg.data(), tbeg.size() * sizeof(int64_t));
+    up(mc.task_end, tend.data(), tend.size() * sizeof(int64_t));
+    up(mc.task_row, trow.data(), trow.size() * sizeof(int32_t));
+    up(mc.task_slot, tslot.data(), tslot.size() * sizeof(int32_t));
+    up(mc.tmulti_row, tmrow.data(), tmrow.size() * sizeof(int32_t));
+    up(mc.tmulti_first, tmfirst.data(), tmfirst.size() * sizeof(int32_t));
+    up(mc.tmulti_count, tmcount.data(), tmcount.size() * sizeof(int32_t));
     DT_CUDA(cudaStreamSynchronize(ctx->stream));
 }
 
@@ -393,6 +724,45 @@ void launch_rows(dt_ctx *ctx, const ModeCopy &mc, int nother, int64_t nnz, const
               mc.val.as<double>(), nnz, nother, mc.rowptr.as<int64_t>(),
               mc.chunk_row.as<int32_t>(), mc.chunk_beg.as<int64_t>(),
               mc.chunk_slot.as<int32_t>(), mc.nchunks, f, P, Yc, Ypart);
+}
+
+template <int RA, int RB, int AW, int BW>
+void launch_t3(dt_ctx *ctx, const ModeCopy &mc, int64_t nnz, const FactorSet &f, double *Yc,
+               double *Ypart) {
+    using C = T3<RA, RB, AW, BW>;
+    const size_t smem = (size_t)T3_WARPS * C::WARP_SMEM * sizeof(double);
+    auto kern = ttmc3_kernel<RA, RB, AW, BW>;
+    DT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int per_sm = std::max<int>(1, std::min<int>(8, (int)((220 * 1024) / smem)));
+    const unsigned blocks = (unsigned)std::max<int64_t>(
+        1, std::min<int64_t>((mc.ntasks + T3_WARPS - 1) / T3_WARPS, (int64_t)per_sm * ctx->num_sms));
+    DT_LAUNCH(ctx, kern, blocks, T3_WARPS * 32, smem, mc.other.as<int32_t>(),
+              mc.other.as<int32_t>() + nnz, mc.val.as<double>(), mc.rowptr.as<int64_t>(),
+              mc.nrows, mc.task_beg.as<int64_t>(), mc.task_end.as<int64_t>(),
+              mc.task_row.as<int32_t>(), mc.task_slot.as<int32_t>(), mc.ntasks, f.U[0], f.U[1],
+              Yc, Ypart);
+}
+
+// The 3-way task kernel for the rank pairs it is instantiated for; false if
+// (Ra, Rb) is not one of them.
+bool ttmc3_dispatch(dt_ctx *ctx, const ModeCopy &mc, int64_t nnz, const FactorSet &f, double *Yc,
+                    double *Ypart) {
+    const int a = f.R[0], b = f.R[1];
+#define DT_T3(RA, RB, AW, BW)                                        \
+    if (a == RA && b == RB) {                                        \
+        launch_t3<RA, RB, AW, BW>(ctx, mc, nnz, f, Yc, Ypart);       \
+        return true;                                                 \
+    }
+    DT_T3(16, 16, 2, 4)
+    DT_T3(8, 8, 1, 2)
+    DT_T3(32, 32, 2, 4)
+    DT_T3(16, 8, 1, 4)
+    DT_T3(8, 16, 1, 4)
+    DT_T3(10, 10, 1, 2)
+    DT_T3(12, 12, 1, 4)
+    DT_T3(4, 4, 1, 2)
+#undef DT_T3
+    return false;
 }
 
 }  // namespace
@@ -413,6 +783,25 @@ void sp_ttmc_compact(dt_ctx *ctx, const dt_sptensor *sp, const double *const *Ut
         f.U[d] = Ut_dev[m];
         f.R[d] = (int)R[m];
         d++;
+    }
+    if (nd == 3 && mc.ntasks > 0) {
+        DevMem tpart(ctx, std::max<int64_t>(mc.tslots, 1) * P * sizeof(double));
+        if (timer) timer->begin();
+        if (ttmc3_dispatch(ctx, mc, sp->nnz, f, Yc, tpart.as<double>())) {
+            if (mc.tmulti > 0) {
+                const unsigned blocks = (unsigned)std::min<int64_t>(mc.tmulti, 65535);
+                DT_LAUNCH(ctx, combine_partials_kernel, blocks, 256, 0, tpart.as<double>(),
+                          mc.tmulti_row.as<int32_t>(), mc.tmulti_first.as<int32_t>(),
+                          mc.tmulti_count.as<int32_t>(), mc.tmulti, P, Yc);
+            }
+            if (timer) {
+                double bytes = (double)sp->nnz * (4.0 * (nd - 1) + 8.0) + (double)mc.nrows * P * 8.0;
+                for (int m = 0; m < nd; m++)
+                    if (m != mode) bytes += (double)sp->shape[m] * R[m] * 8.0;
+                timer->end(bytes);
+            }
+            return;
+        }
     }
     DevMem part(ctx, std::max<int64_t>(mc.nslots, 1) * P * sizeof(double));
     if (timer) timer->begin();
@@ -458,8 +847,15 @@ void sp_mtr(dt_ctx *ctx, const dt_sptensor *sp, const double *Yc, int mode, int 
     const int64_t rpb = std::max<int64_t>(64, (mc.nrows + target - 1) / target);
     const int nblk = (int)std::max<int64_t>(1, (mc.nrows + rpb - 1) / rpb);
     DevMem part(ctx, (size_t)nblk * P * Rn * sizeof(double));
-    DT_LAUNCH(ctx, mtr_partial_kernel, nblk, 256, 32 * Rn * sizeof(double), Yc,
-              mc.rows.as<int32_t>(), mc.nrows, P, Un, Rn, rpb, part.as<double>());
+    const int ntl = (Rn + 7) / 8;
+#define DT_MTR(N)                                                                          \
+    DT_LAUNCH(ctx, mtr_mma_kernel<N>, nblk, 256, 0, Yc, mc.rows.as<int32_t>(), mc.nrows, P, \
+              Un, Rn, rpb, part.as<double>())
+    if (ntl == 1) DT_MTR(1);
+    else if (ntl == 2) DT_MTR(2);
+    else if (ntl == 3) DT_MTR(3);
+    else DT_MTR(4);
+#undef DT_MTR
     const int64_t n = (int64_t)P * Rn;
     DT_LAUNCH(ctx, sum_blocks_kernel, std::max(1u, ceil_div(n, 256)), 256, 0,
               part.as<double>(), nblk, n, L);
@@ -468,15 +864,43 @@ void sp_mtr(dt_ctx *ctx, const dt_sptensor *sp, const double *Yc, int mode, int 
 void sp_mtl(dt_ctx *ctx, const dt_sptensor *sp, const double *Yc, int mode, int P,
             const double *L, int Rn, double *out) {
     const ModeCopy &mc = sp->modes[mode];
+    DT_CHECK_ARG(Rn <= 32, "sparse ttmc_mTL: R_n (%d) must be <= 32", Rn);
     DT_CUDA(cudaMemsetAsync(out, 0, sp->shape[mode] * Rn * sizeof(double), ctx->stream));
-    const size_t smem = (size_t)P * Rn * sizeof(double);
-    DT_CHECK_ARG(smem <= 200 * 1024, "sparse ttmc_mTL: L (%d x %d) too large", P, Rn);
-    DT_CUDA(cudaFuncSetAttribute(mtl_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
-    const unsigned blocks =
-        std::max(1u, std::min<unsigned>(ceil_div(mc.nrows, 8), 8u * (unsigned)ctx->num_sms));
-    DT_LAUNCH(ctx, mtl_kernel, blocks, 256, smem, Yc, mc.rows.as<int32_t>(), mc.nrows, P, L,
-              Rn, out);
+    const int ntl = (Rn + 7) / 8;
+    const size_t smem = (size_t)((P + 3) & ~3) * (8 * ntl + 4) * sizeof(double);
+    const bool lsm = smem <= 160 * 1024;
+    const unsigned blocks = std::max(
+        1u, std::min<unsigned>(ceil_div((mc.nrows + 7) / 8, 8), 4u * (unsigned)ctx->num_sms));
+#define DT_MTL(N, S)                                                                         \
+    do {                                                                                     \
+        auto kern = mtl_mma_kernel<N, S>;                                                    \
+        const size_t sm = S ? smem : 0;                                                      \
+        DT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,      \
+                                     (int)sm));                                              \
+        DT_LAUNCH(ctx, kern, blocks, 256, sm, Yc, mc.rows.as<int32_t>(), mc.nrows, P, L, Rn, \
+                  out);                                                                      \
+    } while (0)
+    if (lsm) {
+        if (ntl == 1) DT_MTL(1, true);
+        else if (ntl == 2) DT_MTL(2, true);
+        else if (ntl == 3) DT_MTL(3, true);
+        else DT_MTL(4, true);
+    } else {
+        if (ntl == 1) DT_MTL(1, false);
+        else if (ntl == 2) DT_MTL(2, false);
+        else if (ntl == 3) DT_MTL(3, false);
+        else DT_MTL(4, false);
+    }
+#undef DT_MTL
+}
+
+void detach_sptensors(dt_ctx *ctx) {
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (dt_sptensor *sp : ctx->sptensors) {
+        sp->modes.clear();
+        sp->ctx = nullptr;
+    }
+    ctx->sptensors.clear();
 }
 
 }  // namespace dt
@@ -505,6 +929,8 @@ void upload_factors(dt_ctx *ctx, const dt_sptensor *sp, const double *const *Ut,
 void check_sp(const dt_ctx *ctx, const dt_sptensor *sp, int mode) {
     check_ctx(ctx);
     DT_CHECK_ARG(sp, "null dt_sptensor");
+    DT_CHECK_ARG(sp->ctx == ctx, sp->ctx ? "dt_sptensor belongs to another dt_ctx"
+                                         : "dt_sptensor's dt_ctx was destroyed");
     DT_CHECK_ARG(mode >= 0 && mode < sp->ndim, "sparse: mode %d out of range", mode);
 }
 
@@ -563,6 +989,7 @@ int dt_sptensor_create(dt_ctx *ctx, int64_t nnz, int ndim, const int64_t *const 
             delete sp;
             throw;
         }
+        ctx->sptensors.insert(sp);
         *out = sp;
     });
 }
@@ -570,8 +997,11 @@ int dt_sptensor_create(dt_ctx *ctx, int64_t nnz, int ndim, const int64_t *const 
 int dt_sptensor_destroy(dt_sptensor *sp) {
     return guard([&] {
         if (!sp) return;
-        cudaSetDevice(sp->ctx->device);
-        cudaStreamSynchronize(sp->ctx->stream);
+        if (sp->ctx) {
+            cudaSetDevice(sp->ctx->device);
+            cudaStreamSynchronize(sp->ctx->stream);
+            sp->ctx->sptensors.erase(sp);
+        }
         delete sp;
     });
 }

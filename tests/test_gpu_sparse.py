@@ -25,7 +25,8 @@ def _factors(shape, R, seed):
     return datasets.random_orthonormal_transposed(shape, R, seed)
 
 
-@pytest.mark.parametrize("R", [(16, 16, 16), (8, 4, 2), (5, 3, 7)])
+@pytest.mark.parametrize("R", [(16, 16, 16), (8, 4, 2), (5, 3, 7), (8, 16, 16), (16, 8, 8),
+                               (32, 32, 32), (10, 10, 10), (12, 12, 12), (4, 4, 4)])
 def test_ttmc_rows_mtr_mtl(ctx, oracle_sparse, zipf_small, R):
     idx, vals, shape = zipf_small
     sp = ctx.sptensor(idx, vals, shape)
@@ -91,3 +92,17 @@ def test_out_of_range_index_is_rejected(ctx):
     with pytest.raises(DTError) as e:
         ctx.sptensor(idx, np.array([1.0, 2.0]), [5, 4])
     assert e.value.code == 1
+
+
+def test_sptensor_outlives_its_context(oracle_sparse):
+    """Destroying a context first detaches its sparse tensors: later calls fail
+    with an error and closing the tensor is safe."""
+    from diana_tucker_b200 import Context, DTError, datasets
+    idx, vals, shape = datasets.sparse_zipf((50, 40, 30), 500, alpha=1.1, seed=5)
+    c2 = Context(0)
+    sp = c2.sptensor(idx, vals, shape)
+    c2.close()
+    with pytest.raises(DTError) as e:
+        sp.ttmc_rows(_factors(shape, (2, 2, 2), 6), (2, 2, 2), 0)
+    assert e.value.code == 1
+    sp.close()
