@@ -335,18 +335,15 @@ void launch_batched(dt_ctx *ctx, int nt, const BatchArgs &a, unsigned grid) {
     DT_CUDA(cudaMemsetAsync(a.queue, 0, sizeof(int), ctx->stream));
     switch (nt) {
         case 128:
-            DT_CUDA(cudaFuncSetAttribute(batched_hooi_kernel<128>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            smem_limit(ctx, batched_hooi_kernel<128>, smem);
             DT_LAUNCH(ctx, batched_hooi_kernel<128>, grid, 128, smem, a);
             break;
         case 512:
-            DT_CUDA(cudaFuncSetAttribute(batched_hooi_kernel<512>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            smem_limit(ctx, batched_hooi_kernel<512>, smem);
             DT_LAUNCH(ctx, batched_hooi_kernel<512>, grid, 512, smem, a);
             break;
         default:
-            DT_CUDA(cudaFuncSetAttribute(batched_hooi_kernel<256>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            smem_limit(ctx, batched_hooi_kernel<256>, smem);
             DT_LAUNCH(ctx, batched_hooi_kernel<256>, grid, 256, smem, a);
             break;
     }
@@ -497,16 +494,13 @@ int dt_hooi_batched(dt_ctx *ctx, int count, const int64_t *shapes, const int64_t
         const size_t smem = batched_smem();
         switch (nt) {
             case 128:
-                DT_CUDA(cudaFuncSetAttribute(batched_hooi_kernel<128>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                smem_limit(ctx, batched_hooi_kernel<128>, smem);
                 break;
             case 512:
-                DT_CUDA(cudaFuncSetAttribute(batched_hooi_kernel<512>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                smem_limit(ctx, batched_hooi_kernel<512>, smem);
                 break;
             default:
-                DT_CUDA(cudaFuncSetAttribute(batched_hooi_kernel<256>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                smem_limit(ctx, batched_hooi_kernel<256>, smem);
         }
         cudaMemsetAsync(a.queue, 0, sizeof(int), ctx->stream);
         if (nt == 128)

@@ -69,6 +69,37 @@ void clear_last_error();
         DT_CUDA(cudaGetLastError());                                       \
     } while (0)
 
+// Programmatic dependent launch.  A kernel launched with DT_LAUNCH_PDL may
+// start while the previous kernel in the stream is still running: it must run
+// pdl_wait() before it reads anything that kernel writes (and before it
+// writes anything that kernel reads), and it may do set-up work (barriers,
+// TMEM, shared-memory zeroing) before that.  pdl_trigger() lets the next
+// kernel start its own set-up; every kernel of the sweep calls it early.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <class... KArgs, class... Args>
+void launch_pdl(dt_ctx *ctx, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                Args &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    DT_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...));
+    ctx->launches++;
+}
+
+#define DT_LAUNCH_PDL(ctx, kernel, grid, block, smem, ...) \
+    ::dt::launch_pdl((ctx), (kernel), dim3(grid), dim3(block), (smem), __VA_ARGS__)
+
 // Runs fn() and converts a thrown dt::Error into a status code.
 template <class F>
 int guard(F &&fn) {
@@ -93,6 +124,14 @@ inline void check_ctx(const dt_ctx *ctx) {
 }
 
 bool is_device_ptr(const void *p);
+
+// Raises a kernel's dynamic shared-memory limit to at least `bytes` on ctx's
+// device; the runtime is called only when the limit has to grow.
+void raise_smem_limit(dt_ctx *ctx, const void *kernel, size_t bytes);
+template <class K>
+inline void smem_limit(dt_ctx *ctx, K *kernel, size_t bytes) {
+    raise_smem_limit(ctx, reinterpret_cast<const void *>(kernel), bytes);
+}
 
 // Frees the device memory of every sparse tensor still attached to ctx and
 // detaches it (called by dt_ctx_destroy).

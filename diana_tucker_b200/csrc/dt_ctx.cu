@@ -1,4 +1,7 @@
 // Context lifetime, error reporting and host/device staging.
+#include <map>
+#include <mutex>
+
 #include "dt_core.cuh"
 
 namespace dt {
@@ -26,6 +29,16 @@ bool is_device_ptr(const void *p) {
         return false;
     }
     return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+void raise_smem_limit(dt_ctx *ctx, const void *kernel, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, size_t> limits;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t &cur = limits[{kernel, ctx->device}];
+    if (bytes <= cur) return;
+    DT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    cur = bytes;
 }
 
 void DevMem::alloc(dt_ctx *ctx, size_t bytes) {

@@ -324,15 +324,11 @@ void ttm_launch(dt_ctx *ctx, const TX *X, int64_t L, int64_t I, int64_t B, const
         2 * TTM_BK * JT * sizeof(double) + 2 * TTM_BP * (TTM_BK + EV) * sizeof(TX);
     auto launch = [&](double *dst) {
         if (rows_ok) {
-            DT_CUDA(cudaFuncSetAttribute(ttm_pipe_kernel<TX, JT, false>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem_rows));
+            smem_limit(ctx, ttm_pipe_kernel<TX, JT, false>, smem_rows);
             DT_LAUNCH(ctx, (ttm_pipe_kernel<TX, JT, false>), grid, TTM_NT, smem_rows, X, L, I, P,
                       M, msj, msi, J, dst, kchunk, ysize);
         } else if (kfast_ok) {
-            DT_CUDA(cudaFuncSetAttribute(ttm_pipe_kernel<TX, JT, true>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem_kfast));
+            smem_limit(ctx, ttm_pipe_kernel<TX, JT, true>, smem_kfast);
             DT_LAUNCH(ctx, (ttm_pipe_kernel<TX, JT, true>), grid, TTM_NT, smem_kfast, X, L, I, P,
                       M, msj, msi, J, dst, kchunk, ysize);
         }

@@ -190,7 +190,9 @@ void DenseHooi::init_factors(double *const *U_user) {
         // hooi_als.tpp:74-81: U_rand(I_n x R_n).randn(); U_n = Q of reduced_QR.
         if (opts.seed != DT_SEED_KEEP) srand(opts.seed);
         // Draw every block in mode order (the reference's order), upload once,
-        // then one batched Householder launch for all modes.
+        // then one batched orthonormalisation launch for all modes (any
+        // orthonormal basis of span(U_rand) gives the same sweeps: the TTM
+        // chain's Gram matrices only see U U^T).
         int64_t total = 0;
         for (int m = 0; m < N; m++) total += I[m] * R[m];
         std::vector<double> h((size_t)total);
@@ -206,7 +208,7 @@ void DenseHooi::init_factors(double *const *U_user) {
             qp[m] = U[m].as<double>();
             off += I[m] * R[m];
         }
-        householder_qr_batch(ctx, N, ap.data(), qp.data(), I, R);
+        orth_batch(ctx, N, ap.data(), qp.data(), I, R);
         return;
     }
     // HOSVD: leading R_n eigenvectors of X_(n) X_(n)^T by subspace iteration

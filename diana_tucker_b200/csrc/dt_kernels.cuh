@@ -49,6 +49,11 @@ void householder_qr(dt_ctx *ctx, const double *A, int64_t m, int64_t n, double *
 void householder_qr_batch(dt_ctx *ctx, int count, const double *const *A, double *const *Q,
                           const int64_t *m, const int64_t *n);
 
+// Orthonormal bases Q[b] of span(A[b]) for a batch (CholeskyQR2 on the FP64
+// tensor-core path, Householder on breakdown or for large matrices).
+void orth_batch(dt_ctx *ctx, int count, const double *const *A, double *const *Q,
+                const int64_t *m, const int64_t *n);
+
 // Orthonormal basis of span(S^iters L) for the n x n symmetric S and the n x r
 // col-major L (in place), one CTA; CholeskyQR2 per step with a Householder
 // fallback.  work >= 3*n*r + r.  Sets *flag bit 2 when a fallback ran.

@@ -387,6 +387,13 @@ __global__ void __launch_bounds__(LA_NT) subspace_kernel(const double *Sg, int64
 // warp 0 (rsqrt per pivot, multiplications by the reciprocal diagonal).  A
 // Cholesky breakdown restarts from the caller's L with Householder steps.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void la_cp_async16(void *smem, const void *gmem) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void la_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void la_cp_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 constexpr int SM_WARPS = 8;
 constexpr int SM_NT = SM_WARPS * 32;
 constexpr int SM_GP = 512;  // doubles of Gram partials (K split only below 8 tiles)
@@ -530,49 +537,57 @@ __device__ __forceinline__ void sm_gram(const double *src, int n, int r, double 
     __syncthreads();
 }
 
-// Warp 0: G = R^T R (R upper), Ri = R^{-1} (row-major, pitch LDR).  Lane c
-// holds column c of G / R during the factorisation; R (overwriting G) and the
-// reciprocal diagonal (dinv) then go through shared memory, so the inverse
-// keeps only its own column in registers.  Returns false on a non-positive pivot.
+// G = R^T R (R upper, overwriting the upper triangle of G; the strict lower
+// triangle is zeroed), with the whole CTA: per pivot k every thread reads the
+// pivot and row k, then the threads owning entries (i, j), k < i <= j, update
+// them while the owners of row k scale it.  Two barriers per pivot, no
+// divides.  dinv[k] = 1 / R(k, k) (1 for the padding).  Returns false on a
+// non-positive pivot (the same value in every thread).
 template <int RT>
-__device__ __forceinline__ bool sm_chol_inv(double *G, double *Ri, double *dinv, int r) {
-    constexpr int LDR = SmTile<RT>::LDR;
-    const int lane = threadIdx.x & 31;
-    const bool act = lane < RT;
-    bool ok;
-    {
-        double gc[RT];
+__device__ __forceinline__ bool sm_chol(double *G, double *dinv, int r) {
+    constexpr int EPT = (RT * RT + SM_NT - 1) / SM_NT;
+    const int t = threadIdx.x;
+    const double g00 = G[0];
+    bool ok = g00 > 0.0;
+    for (int k = 0; k < r; k++) {
+        const double d = G[k * RT + k];
+        ok = ok && (d > 1e-28 * g00);
+        const double ri = rsqrt(fmax(d, 1e-300));
+        double upd[EPT];
 #pragma unroll
-        for (int i = 0; i < RT; i++) gc[i] = act ? G[i * RT + lane] : 0.0;
-        const double g00 = __shfl_sync(0xffffffffu, gc[0], 0);
-        ok = g00 > 0.0;
+        for (int q = 0; q < EPT; q++) {
+            const int e = t + q * SM_NT, i = e / RT, j = e % RT;
+            upd[q] = (e < RT * RT && i > k && i <= j && j < r)
+                         ? (G[k * RT + i] * ri) * (G[k * RT + j] * ri)
+                         : 0.0;
+        }
+        __syncthreads();
 #pragma unroll
-        for (int k = 0; k < RT; k++) {
-            if (k < r) {
-                const double d = __shfl_sync(0xffffffffu, gc[k], k);
-                ok = ok && (d > 1e-28 * g00);
-                const double ri = rsqrt(fmax(d, 1e-300));
-                if (lane == k) dinv[k] = ri;
-                if (lane >= k) gc[k] *= ri;
-#pragma unroll
-                for (int i = k + 1; i < RT; i++) {
-                    if (i < r) {
-                        const double rki = __shfl_sync(0xffffffffu, gc[k], i);
-                        if (lane >= i) gc[i] = fma(-rki, gc[k], gc[i]);
-                    }
-                }
-            } else if (lane == k) {
-                dinv[k] = 1.0;
+        for (int q = 0; q < EPT; q++) {
+            const int e = t + q * SM_NT, i = e / RT, j = e % RT;
+            if (e < RT * RT && j < r) {
+                if (i > k && i <= j) G[e] -= upd[q];
+                else if (i == k && j >= k) G[e] *= ri;
             }
         }
-        __syncwarp();
-        if (act) {
-#pragma unroll
-            for (int i = 0; i < RT; i++) G[i * RT + lane] = i <= lane ? gc[i] : 0.0;
-        }
+        if (t == k) dinv[k] = ri;
+        __syncthreads();
     }
-    __syncwarp();
-    // Column `lane` of R^{-1}: x_i = (delta_{i,lane} - sum_{j>i} R(i,j) x_j) / R(i,i).
+    for (int e = t; e < RT * RT; e += SM_NT) {
+        const int i = e / RT, j = e % RT;
+        if (i > j) G[e] = 0.0;
+    }
+    if (t >= r && t < RT) dinv[t] = 1.0;
+    __syncthreads();
+    return ok;
+}
+
+// Warp 0: Ri = R^{-1} (row-major, pitch LDR) from R in the upper triangle of G
+// and dinv.  Lane c solves column c: x_i = (delta_{i,c} - sum_{j>i} R(i,j) x_j) dinv_i.
+template <int RT>
+__device__ __forceinline__ void sm_rinv(const double *G, double *Ri, const double *dinv) {
+    constexpr int LDR = SmTile<RT>::LDR;
+    const int lane = threadIdx.x & 31;
     double x[RT];
 #pragma unroll
     for (int i = RT - 1; i >= 0; i--) {
@@ -587,12 +602,55 @@ __device__ __forceinline__ bool sm_chol_inv(double *G, double *Ri, double *dinv,
         }
         x[i] = (s0 + s1) * dinv[i];
     }
-    if (act) {
+    if (lane < RT) {
 #pragma unroll
         for (int i = 0; i < RT; i++) Ri[i * LDR + lane] = i <= lane ? x[i] : 0.0;
     }
-    __syncwarp();
+}
+
+// Cholesky + R^{-1} (all threads call it; ends with a barrier).
+template <int RT>
+__device__ __forceinline__ bool sm_chol_inv(double *G, double *Ri, double *dinv, int r) {
+    const bool ok = sm_chol<RT>(G, dinv, r);
+    if (threadIdx.x < 32) sm_rinv<RT>(G, Ri, dinv);
+    __syncthreads();
     return ok;
+}
+
+// After one CholeskyQR pass, Q^T Q = I + E with E tiny.  When max |E| <= 1e-8,
+// C = I - E/2 + 3E^2/8 (the series of (I + E)^{-1/2}) makes Q C orthonormal to
+// rounding; C goes to Ri (pitch LDR) for sm_apply.  Returns false when E is too
+// large, and the caller runs a second CholeskyQR pass instead.  All threads.
+template <int RT>
+__device__ __forceinline__ bool sm_polar_fix(const double *G, double *Ri, double *red) {
+    constexpr int LDR = SmTile<RT>::LDR;
+    const int t = threadIdx.x;
+    double emax = 0.0;
+    for (int e = t; e < RT * RT; e += SM_NT) {
+        const int a = e / RT, b = e % RT;
+        emax = fmax(emax, fabs(G[e] - (a == b ? 1.0 : 0.0)));
+    }
+    for (int o = 16; o > 0; o >>= 1) emax = fmax(emax, __shfl_xor_sync(0xffffffffu, emax, o));
+    if ((t & 31) == 0) red[t >> 5] = emax;
+    __syncthreads();
+    double m = 0.0;
+#pragma unroll
+    for (int w = 0; w < SM_WARPS; w++) m = fmax(m, red[w]);
+    if (!(m <= 1e-8)) {
+        __syncthreads();
+        return false;
+    }
+    for (int e = t; e < RT * RT; e += SM_NT) {
+        const int a = e / RT, b = e % RT;
+        double e2 = 0.0;
+#pragma unroll
+        for (int k = 0; k < RT; k++)
+            e2 = fma(G[a * RT + k] - (a == k ? 1.0 : 0.0), G[k * RT + b] - (k == b ? 1.0 : 0.0), e2);
+        const double eab = G[e] - (a == b ? 1.0 : 0.0);
+        Ri[a * LDR + b] = (a == b ? 1.0 : 0.0) - 0.5 * eab + 0.375 * e2;
+    }
+    __syncthreads();
+    return true;
 }
 
 template <int RT>
@@ -616,6 +674,8 @@ __global__ void __launch_bounds__(SM_NT, 1) subspace_mma_kernel(const double *Sg
     __shared__ double red[33];
     __shared__ int bad;
     const int t = threadIdx.x;
+    pdl_trigger();
+    pdl_wait();
     const int n8 = (n + 7) / 8 * 8;
     const int lds = sm_lds(n8);
     double *A = sm;
@@ -626,16 +686,56 @@ __global__ void __launch_bounds__(SM_NT, 1) subspace_mma_kernel(const double *Sg
     double *dinv = Ri + RT * T::LDR;
     double *Ss = dinv + 32;
     if (SMODE == S_FULL) {
-        for (int e = t; e < lds * n8; e += SM_NT) {
-            const int i = e % lds, k = e / lds;
-            Ss[e] = (i < n && k < n) ? Sg[i + n * k] : 0.0;
+        // S goes global -> shared with asynchronous 16-byte copies (one
+        // latency for the whole matrix); the padding is zeroed meanwhile.
+        if ((n & 1) == 0) {
+            const int hc = n / 2;
+            for (int e = t; e < hc * n; e += SM_NT) {
+                const int k = e / hc, q = e - k * hc;
+                la_cp_async16(Ss + lds * k + 2 * q, Sg + (int64_t)n * k + 2 * q);
+            }
+            la_cp_commit();
+        } else {
+            for (int e = t; e < n * n; e += SM_NT) {
+                const int k = e / n, i = e - k * n;
+                Ss[i + lds * k] = Sg[e];
+            }
+        }
+        const int pr = lds - n;
+        for (int e = t; e < pr * n8; e += SM_NT) {
+            const int k = e / pr, i = n + (e - k * pr);
+            Ss[i + lds * k] = 0.0;
+        }
+        for (int e = t; e < (n8 - n) * n; e += SM_NT) {
+            const int k = n + e / n, i = e % n;
+            Ss[i + lds * k] = 0.0;
         }
     }
+    // L (n x r col-major) -> A (row-major, pitch LDQ, zero padded): all loads
+    // of a thread are issued before its stores.
     for (int e = t; e < n8 * T::LDQ; e += SM_NT) {
-        const int i = e / T::LDQ, c = e % T::LDQ;
-        A[e] = (i < n && c < r) ? Lg[i + (int64_t)n * c] : 0.0;
+        A[e] = 0.0;
         B[e] = 0.0;
     }
+    __syncthreads();
+    {
+        constexpr int MAXQ = 32;  // n * r <= 256 * 32 = SM_NT * MAXQ
+        double v[MAXQ];
+#pragma unroll
+        for (int q = 0; q < MAXQ; q++) {
+            const int e = t + SM_NT * q;
+            v[q] = e < n * r ? Lg[e] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < MAXQ; q++) {
+            const int e = t + SM_NT * q;
+            if (e < n * r) {
+                const int c = e / n, i = e - c * n;
+                A[i * T::LDQ + c] = v[q];
+            }
+        }
+    }
+    if (SMODE == S_FULL && (n & 1) == 0) la_cp_wait_all();
     if (t == 0) bad = 0;
     __syncthreads();
 
@@ -651,12 +751,13 @@ __global__ void __launch_bounds__(SM_NT, 1) subspace_mma_kernel(const double *Sg
             const int passes = last ? 2 : 1;
             for (int p = 0; p < passes; p++) {
                 sm_gram<RT>(cur, n, r, Gp, G);
-                if (t < 32) {
-                    const bool ok = sm_chol_inv<RT>(G, Ri, dinv, r);
-                    if (t == 0 && !ok) bad = 1;
+                // The second pass is usually a tiny correction (polar fix).
+                if (!(p == 1 && sm_polar_fix<RT>(G, Ri, red))) {
+                    if (!sm_chol_inv<RT>(G, Ri, dinv, r)) {
+                        bad = 1;
+                        break;
+                    }
                 }
-                __syncthreads();
-                if (bad) break;
                 sm_apply<RT>(cur, Ri, n8, oth);
                 __syncthreads();
                 tmp = cur;
@@ -696,13 +797,68 @@ __global__ void __launch_bounds__(SM_NT, 1) subspace_mma_kernel(const double *Sg
     for (int e = t; e < n * r; e += SM_NT) Lg[e] = Lw[e];
 }
 
+// Q[b] = orth(A[b]) for a batch of m x n (n <= RT) col-major matrices, one CTA
+// each: CholeskyQR2 with the mma.sync Gram / apply above; a Cholesky
+// breakdown falls back to Householder on work[b] (m n + n doubles).  The span
+// is that of A, as with Householder QR; the basis may differ by a rotation.
+template <int RT>
+__global__ void __launch_bounds__(SM_NT, 1) cholqr2_batch_kernel(const double *const *A,
+                                                                double *const *Q,
+                                                                const int64_t *m,
+                                                                const int64_t *n,
+                                                                double *const *work) {
+    using T = SmTile<RT>;
+    extern __shared__ __align__(16) double sm[];
+    __shared__ double red[33];
+    __shared__ int bad;
+    const int b = blockIdx.x, t = threadIdx.x;
+    const int M = (int)m[b], r = (int)n[b];
+    const int M8 = (M + 7) / 8 * 8;
+    double *Z0 = sm;
+    double *Z1 = Z0 + M8 * T::LDQ;
+    double *Gp = Z1 + M8 * T::LDQ;
+    double *G = Gp + SM_GP;
+    double *Ri = G + RT * RT;
+    double *dinv = Ri + RT * T::LDR;
+    for (int e = t; e < M8 * T::LDQ; e += SM_NT) {
+        const int i = e / T::LDQ, c = e % T::LDQ;
+        Z0[e] = (i < M && c < r) ? A[b][i + (int64_t)M * c] : 0.0;
+    }
+    if (t == 0) bad = 0;
+    __syncthreads();
+    double *cur = Z0, *oth = Z1;
+    for (int p = 0; p < 2; p++) {
+        sm_gram<RT>(cur, M, r, Gp, G);
+        if (!sm_chol_inv<RT>(G, Ri, dinv, r)) {
+            bad = 1;
+            break;
+        }
+        sm_apply<RT>(cur, Ri, M8, oth);
+        __syncthreads();
+        double *tmp = cur;
+        cur = oth;
+        oth = tmp;
+    }
+    if (!bad) {
+        for (int e = t; e < M * r; e += SM_NT) {
+            const int i = e % M, c = e / M;
+            Q[b][e] = cur[i * T::LDQ + c];
+        }
+        return;
+    }
+    double *W = work[b];
+    for (int e = t; e < M * r; e += SM_NT) W[e] = A[b][e];
+    __syncthreads();
+    hqr_device(W, M, r, W + (int64_t)M * r, Q[b], red);
+}
+
 template <int RT, int SMODE>
 void launch_subspace_mma(dt_ctx *ctx, const double *S, int n, double *L, int r, int iters,
                          double *work, int *flag) {
     const size_t smem = sm_smem_doubles<RT>(n, SMODE == S_FULL) * sizeof(double);
     auto kern = subspace_mma_kernel<RT, SMODE>;
-    DT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    DT_LAUNCH(ctx, kern, 1, SM_NT, smem, S, n, L, r, iters, work, flag);
+    smem_limit(ctx, kern, smem);
+    DT_LAUNCH_PDL(ctx, kern, 1, SM_NT, smem, S, n, L, r, iters, work, flag);
 }
 
 template <int RT>
@@ -930,6 +1086,58 @@ void householder_qr(dt_ctx *ctx, const double *A, int64_t m, int64_t n, double *
     DT_LAUNCH(ctx, hqr_kernel, 1, LA_NT, 0, A, m, n, Q, R, work);
 }
 
+void orth_batch(dt_ctx *ctx, int count, const double *const *A, double *const *Q,
+                const int64_t *m, const int64_t *n) {
+    int64_t maxm = 0, maxn = 0;
+    for (int b = 0; b < count; b++) {
+        DT_CHECK_ARG(m[b] >= n[b] && n[b] > 0, "orth_batch: need m >= n > 0");
+        maxm = std::max(maxm, m[b]);
+        maxn = std::max(maxn, n[b]);
+    }
+    const int RT = maxn <= 8 ? 8 : (maxn <= 16 ? 16 : 32);
+    const int64_t M8 = (maxm + 7) / 8 * 8;
+    const size_t smem =
+        (2 * (size_t)M8 * (RT + 4) + SM_GP + RT * RT + RT * (RT + 4) + 32) * sizeof(double);
+    if (maxn > 32 || smem > 220 * 1024) {
+        householder_qr_batch(ctx, count, A, Q, m, n);
+        return;
+    }
+    std::vector<const double *> hA(A, A + count);
+    std::vector<double *> hQ(Q, Q + count), hW(count);
+    std::vector<int64_t> hm(m, m + count), hn(n, n + count);
+    std::vector<DevMem> ws(count);
+    for (int b = 0; b < count; b++) {
+        ws[b].alloc(ctx, (m[b] * n[b] + n[b]) * sizeof(double));
+        hW[b] = ws[b].as<double>();
+    }
+    DevMem tab(ctx, count * (3 * sizeof(void *) + 2 * sizeof(int64_t)));
+    char *base = static_cast<char *>(tab.get());
+    const size_t pb = count * sizeof(void *);
+    DT_CUDA(cudaMemcpyAsync(base, hA.data(), pb, cudaMemcpyHostToDevice, ctx->stream));
+    DT_CUDA(cudaMemcpyAsync(base + pb, hQ.data(), pb, cudaMemcpyHostToDevice, ctx->stream));
+    DT_CUDA(cudaMemcpyAsync(base + 2 * pb, hW.data(), pb, cudaMemcpyHostToDevice, ctx->stream));
+    DT_CUDA(cudaMemcpyAsync(base + 3 * pb, hm.data(), count * sizeof(int64_t),
+                            cudaMemcpyHostToDevice, ctx->stream));
+    DT_CUDA(cudaMemcpyAsync(base + 3 * pb + count * sizeof(int64_t), hn.data(),
+                            count * sizeof(int64_t), cudaMemcpyHostToDevice, ctx->stream));
+    const auto *tA = reinterpret_cast<const double *const *>(base);
+    auto *tQ = reinterpret_cast<double *const *>(base + pb);
+    auto *tW = reinterpret_cast<double *const *>(base + 2 * pb);
+    const auto *tm = reinterpret_cast<const int64_t *>(base + 3 * pb);
+    const auto *tn = reinterpret_cast<const int64_t *>(base + 3 * pb + count * sizeof(int64_t));
+#define DT_CQR(R)                                                                            \
+    do {                                                                                     \
+        auto kern = cholqr2_batch_kernel<R>;                                                 \
+        smem_limit(ctx, kern, smem);                                                         \
+        DT_LAUNCH(ctx, kern, count, SM_NT, smem, tA, tQ, tm, tn, tW);                        \
+    } while (0)
+    if (RT == 8) DT_CQR(8);
+    else if (RT == 16) DT_CQR(16);
+    else DT_CQR(32);
+#undef DT_CQR
+    DT_CUDA(cudaStreamSynchronize(ctx->stream));  // host tables go out of scope
+}
+
 void householder_qr_batch(dt_ctx *ctx, int count, const double *const *A, double *const *Q,
                           const int64_t *m, const int64_t *n) {
     // Pointer and size tables plus per-matrix workspaces, staged to the device.
@@ -994,13 +1202,11 @@ void subspace_iter(dt_ctx *ctx, const double *S, int64_t n, double *L, int64_t r
     const int zl_in = base + s_bytes + zl_bytes <= cap;
     const size_t smem = base + s_bytes + (zl_in ? zl_bytes : 0);
     if (r <= 16) {
-        DT_CUDA(cudaFuncSetAttribute(subspace_kernel<16>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        smem_limit(ctx, subspace_kernel<16>, smem);
         DT_LAUNCH(ctx, subspace_kernel<16>, 1, LA_NT, smem, S, n, L, r, iters, work, s_mode,
                   zl_in, flag);
     } else {
-        DT_CUDA(cudaFuncSetAttribute(subspace_kernel<32>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        smem_limit(ctx, subspace_kernel<32>, smem);
         DT_LAUNCH(ctx, subspace_kernel<32>, 1, LA_NT, smem, S, n, L, r, iters, work, s_mode,
                   zl_in, flag);
     }

@@ -732,7 +732,7 @@ void launch_t3(dt_ctx *ctx, const ModeCopy &mc, int64_t nnz, const FactorSet &f,
     using C = T3<RA, RB, AW, BW>;
     const size_t smem = (size_t)T3_WARPS * C::WARP_SMEM * sizeof(double);
     auto kern = ttmc3_kernel<RA, RB, AW, BW>;
-    DT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    smem_limit(ctx, kern, smem);
     const int per_sm = std::max<int>(1, std::min<int>(8, (int)((220 * 1024) / smem)));
     const unsigned blocks = (unsigned)std::max<int64_t>(
         1, std::min<int64_t>((mc.ntasks + T3_WARPS - 1) / T3_WARPS, (int64_t)per_sm * ctx->num_sms));
@@ -875,8 +875,7 @@ void sp_mtl(dt_ctx *ctx, const dt_sptensor *sp, const double *Yc, int mode, int 
     do {                                                                                     \
         auto kern = mtl_mma_kernel<N, S>;                                                    \
         const size_t sm = S ? smem : 0;                                                      \
-        DT_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,      \
-                                     (int)sm));                                              \
+        smem_limit(ctx, kern, sm);                                                           \
         DT_LAUNCH(ctx, kern, blocks, 256, sm, Yc, mc.rows.as<int32_t>(), mc.nrows, P, L, Rn, \
                   out);                                                                      \
     } while (0)

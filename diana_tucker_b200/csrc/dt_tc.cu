@@ -92,6 +92,7 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * S + 4);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    pdl_trigger();
     if (warp == 1) {
         tmem_alloc(tmem_slot, a.tmem_cols);
         tmem_relinquish();
@@ -107,6 +108,9 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
         }
         fence_mbar_init();
     }
+    // Everything above is private set-up; U and the input tensor may still be
+    // in flight from the previous kernel.
+    pdl_wait();
     // B = [U_hi | U_lo]^T (split) or U_hi^T, K-major, 128B-swizzled, zero padded.
     {
         const int kmax = a.kchunks * KC_ELEMS;
@@ -314,6 +318,7 @@ __global__ void __launch_bounds__(128, 1)
     uint64_t *full = bars, *done = bars + nck;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + nck + 1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    pdl_trigger();
     if (warp == 0) {
         tmem_alloc(tmem_slot, a.tmem_cols);
         tmem_relinquish();
@@ -332,6 +337,7 @@ __global__ void __launch_bounds__(128, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
+    pdl_wait();  // Y_(n) and the partial buffer are shared with earlier kernels
     bool ok = true;
     if (threadIdx.x == 0) {
         for (int c = 0; c < n_my; c++) {
@@ -359,22 +365,24 @@ __global__ void __launch_bounds__(128, 1)
     __syncthreads();
     if (n_my > 0 && mbar_wait(done, 0, a.err)) {
         tc_fence_after();
+        // Partial tile stored column-major (element (m, g) at g * Ipad + m):
+        // lane m of a warp writes consecutive addresses for every column.
         const int m = warp * 32 + lane;
-        float *dst = a.part + (int64_t)blockIdx.x * a.Ipad * a.N + (int64_t)m * a.N;
+        float *dst = a.part + (int64_t)blockIdx.x * a.Ipad * a.N + m;
         for (int g = 0; g < a.N; g += 16) {
             float v[16];
             tmem_ld16(tmem_base + ((uint32_t)(warp * 32) << 16) + g, v);
             tmem_wait_ld();
             if (m < a.Ipad) {
 #pragma unroll
-                for (int i = 0; i < 16; i++) dst[g + i] = v[i];
+                for (int i = 0; i < 16; i++) dst[(int64_t)(g + i) * a.Ipad] = v[i];
             }
         }
     } else if (n_my == 0) {
         const int m = warp * 32 + lane;
         if (m < a.Ipad)
             for (int g = 0; g < a.N; g++)
-                a.part[(int64_t)blockIdx.x * a.Ipad * a.N + (int64_t)m * a.N + g] = 0.f;
+                a.part[(int64_t)blockIdx.x * a.Ipad * a.N + (int64_t)g * a.Ipad + m] = 0.f;
     }
     tc_fence_before();
     __syncthreads();
@@ -384,16 +392,19 @@ __global__ void __launch_bounds__(128, 1)
     }
 }
 
-// S[i + n*j] = sum_z part[z][i][j] (+ part[z][i][Ipad+j] + part[z][j][Ipad+i]).
+// S[i + n*j] = sum_z P_z(i, j) (+ P_z(i, Ipad+j) + P_z(j, Ipad+i)), with the
+// partial tiles column-major: P_z(m, g) = part[z][g * Ipad + m].
 __global__ void gram_reduce_kernel(const float *__restrict__ part, int nz, int n, int Ipad, int N,
                                    int split, double *__restrict__ S) {
+    pdl_trigger();
+    pdl_wait();
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n * n; e += gridDim.x * blockDim.x) {
         const int i = e % n, j = e / n;
         double s = 0.0;
         for (int z = 0; z < nz; z++) {
             const float *p = part + (int64_t)z * Ipad * N;
-            s += (double)p[i * N + j];
-            if (split) s += (double)p[i * N + Ipad + j] + (double)p[j * N + Ipad + i];
+            s += (double)p[j * Ipad + i];
+            if (split) s += (double)p[(Ipad + j) * Ipad + i] + (double)p[(Ipad + i) * Ipad + j];
         }
         S[e] = s;
     }
@@ -601,9 +612,8 @@ void tc_ttm(dt_ctx *ctx, const __nv_bfloat16 *Xh, const __nv_bfloat16 *Xl, int64
     const bool folded = om.nl == 1 && om.nb == 1 && om.dl[0] == std::max<int64_t>(L, 1) &&
                         om.sl[0] == 1 && om.sb[0] == L * J && om.jstride == L;
     auto go = [&](auto kernel) {
-        DT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
-        DT_LAUNCH(ctx, kernel, grid, TTM_THREADS, smem, mh, ml, a);
+        smem_limit(ctx, kernel, smem);
+        DT_LAUNCH_PDL(ctx, kernel, grid, TTM_THREADS, smem, mh, ml, a);
     };
     if (a.Jpad == 16) {
         if (a.split) folded ? go(tc_ttm_kernel<16, true, true>) : go(tc_ttm_kernel<16, true, false>);
@@ -649,11 +659,10 @@ void tc_gram(dt_ctx *ctx, const __nv_bfloat16 *Yh, const __nv_bfloat16 *Yl, int6
     CUtensorMap mh = make_map(Yh, 2, dims, str, box);
     CUtensorMap ml = Yl ? make_map(Yl, 2, dims, str, box) : mh;
     const size_t smem = 1024 + (size_t)nck * a.chunk_bytes + (nck + 2) * 8 + 16;
-    DT_CUDA(cudaFuncSetAttribute(tc_gram_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
-    DT_LAUNCH(ctx, tc_gram_kernel, (unsigned)nz, 128, smem, mh, ml, a);
+    smem_limit(ctx, tc_gram_kernel, smem);
+    DT_LAUNCH_PDL(ctx, tc_gram_kernel, (unsigned)nz, 128, smem, mh, ml, a);
     const int n = (int)I;
-    DT_LAUNCH(ctx, gram_reduce_kernel, std::max(1u, ceil_div((int64_t)n * n, 256)), 256, 0,
+    DT_LAUNCH_PDL(ctx, gram_reduce_kernel, std::max(1u, ceil_div((int64_t)n * n, 256)), 256, 0,
               a.part, (int)nz, n, a.Ipad, a.N, a.split, S);
 }
 
