@@ -66,6 +66,9 @@ def _alloc_like(ref_is_torch, shape, dtype=np.float64, device=None):
     return np.zeros(shape, dtype=dtype, order="F")
 
 
+_CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy
+
+
 class Context:
     """A dt_ctx bound to one GPU (dt_ctx_create)."""
 
@@ -100,6 +103,10 @@ class Context:
         if any(_is_torch(o) for o in objs):
             import torch
             s = torch.cuda.current_stream(self.device).cuda_stream
+            # Handle 0 is torch's legacy default stream; NULL would select the
+            # context's own (non-blocking) stream, so pass cudaStreamLegacy.
+            if s == 0:
+                s = _CUDA_STREAM_LEGACY
             if s != self._torch_stream:
                 _lib.check(self.lib.dt_ctx_set_stream(self.h, ctypes.c_void_p(s)))
                 self._torch_stream = s
@@ -292,6 +299,64 @@ class Context:
                                           ctypes.c_void_p(G.ctypes.data) if G is not None else None,
                                           Uptr, ctypes.byref(rep)))
         return G, U, rep.as_dict()
+
+    # -- learned warm start ------------------------------------------------------
+    def ws_loss_grad(self, U, E, D):
+        """Autoencoder loss |D E U - U|^2 / N and its gradients (dt_ws_loss_grad).
+        U: n x N, E: k x n, D: n x k (numpy, float64).  Returns (loss, gE, gD)."""
+        self._bind()
+        U = np.asfortranarray(U, dtype=np.float64)
+        E = np.asfortranarray(E, dtype=np.float64)
+        D = np.asfortranarray(D, dtype=np.float64)
+        n, N = U.shape
+        k = E.shape[0]
+        loss = np.zeros(1)
+        gE = np.zeros((k, n), order="F")
+        gD = np.zeros((n, k), order="F")
+        _lib.check(self.lib.dt_ws_loss_grad(self.h, U.ctypes.data, n, N, k, E.ctypes.data,
+                                            D.ctypes.data, loss.ctypes.data, gE.ctypes.data,
+                                            gD.ctypes.data))
+        return float(loss[0]), gE, gD
+
+    def ws_train(self, U, k, steps=400, lr=0.02, seed=1):
+        """Trains the warm-start autoencoder on the columns of U (n x N).
+        Returns (E, D, loss history)."""
+        self._bind()
+        U = np.asfortranarray(U, dtype=np.float64)
+        n, N = U.shape
+        E = np.zeros((k, n), order="F")
+        D = np.zeros((n, k), order="F")
+        hist = np.zeros(max(steps, 1))
+        _lib.check(self.lib.dt_ws_train(self.h, U.ctypes.data, n, N, k, steps, lr, seed,
+                                        E.ctypes.data, D.ctypes.data, hist.ctypes.data))
+        return E, D, hist[:steps]
+
+    def ws_init(self, X, ranks, D, shape=None, sketch_sweeps=0):
+        """Warm-start factors for dense HOOI from decoder D (dt_ws_init).
+        X: numpy or torch (float32/float64, column-major).  Returns
+        (U list, fit of the sketch, fit of the initial factors)."""
+        self._bind(X)
+        if _is_torch(X):
+            import torch
+            dtype = _lib.DT_F64 if X.dtype == torch.float64 else _lib.DT_F32
+            xptr = ctypes.c_void_p(X.data_ptr())
+            shape = list(shape) if shape is not None else list(X.shape)
+        else:
+            X = np.asfortranarray(X)
+            dtype = _lib.DT_F64 if X.dtype == np.float64 else _lib.DT_F32
+            xptr = ctypes.c_void_p(X.ctypes.data)
+            shape = list(X.shape)
+        D = np.asfortranarray(D, dtype=np.float64)
+        k = D.shape[1]
+        N = len(shape)
+        U = [np.zeros((shape[m], ranks[m]), order="F") for m in range(N)]
+        Uptr = (ctypes.c_void_p * N)(*[u.ctypes.data for u in U])
+        fs, fi = ctypes.c_double(), ctypes.c_double()
+        s, r = _shape_arr(shape), _shape_arr(ranks)
+        _lib.check(self.lib.dt_ws_init(self.h, xptr, dtype, N, _i64p(s), _i64p(r),
+                                       D.ctypes.data, k, int(sketch_sweeps), Uptr,
+                                       ctypes.byref(fs), ctypes.byref(fi)))
+        return U, fs.value, fi.value
 
     # -- batched ---------------------------------------------------------------
     def hooi_batched(self, tensors, ranks, U0, sweeps=10, inner_iters=5, block_threads=0):

@@ -103,6 +103,12 @@ _SIGS = [
     ("dt_ttm_f64", ctypes.c_int, [_vp, _vp, ctypes.c_int, c_i64p, ctypes.c_int, _vp,
                                   ctypes.c_int64, _vp]),
     ("dt_gram_f64", ctypes.c_int, [_vp, _vp, ctypes.c_int, c_i64p, ctypes.c_int, _vp]),
+    ("dt_ws_loss_grad", ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
+                                       _vp, _vp, _vp, _vp, _vp]),
+    ("dt_ws_train", ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_double, ctypes.c_uint64, _vp, _vp, _vp]),
+    ("dt_ws_init", ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, c_i64p, c_i64p, _vp,
+                                  ctypes.c_int, ctypes.c_int, _vp, c_dp, c_dp]),
     ("dt_gram_f64_noalloc", ctypes.c_int, [_vp, _vp, ctypes.c_int, c_i64p, ctypes.c_int,
                                            _vp]),
     ("dt_ttt_except_f64", ctypes.c_int, [_vp, _vp, c_i64p, _vp, c_i64p, ctypes.c_int,

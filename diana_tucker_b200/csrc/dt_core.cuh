@@ -80,6 +80,10 @@ __device__ __forceinline__ void pdl_trigger() {
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
+// DT_DISABLE_PDL=1 in the environment launches these kernels in plain
+// stream order (for diagnosis).
+bool pdl_enabled();
+
 template <class... KArgs, class... Args>
 void launch_pdl(dt_ctx *ctx, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
                 Args &&...args) {
@@ -92,7 +96,9 @@ void launch_pdl(dt_ctx *ctx, void (*kernel)(KArgs...), dim3 grid, dim3 block, si
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    const bool plain_stream = ctx->stream != nullptr && ctx->stream != cudaStreamLegacy &&
+                              ctx->stream != cudaStreamPerThread;
+    cfg.numAttrs = pdl_enabled() && plain_stream ? 1 : 0;
     DT_CUDA(cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...));
     ctx->launches++;
 }

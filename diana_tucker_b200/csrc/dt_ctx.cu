@@ -1,4 +1,5 @@
 // Context lifetime, error reporting and host/device staging.
+#include <cstdlib>
 #include <map>
 #include <mutex>
 
@@ -29,6 +30,14 @@ bool is_device_ptr(const void *p) {
         return false;
     }
     return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+bool pdl_enabled() {
+    static const bool on = [] {
+        const char *e = std::getenv("DT_DISABLE_PDL");
+        return !(e && e[0] == '1');
+    }();
+    return on;
 }
 
 void raise_smem_limit(dt_ctx *ctx, const void *kernel, size_t bytes) {

@@ -100,7 +100,8 @@ typedef struct {
 DT_API int dt_ctx_create(int device, dt_ctx **ctx);
 DT_API int dt_ctx_destroy(dt_ctx *ctx);
 /* Run all work of this context on the given cudaStream_t (NULL = the
- * context's own stream). */
+ * context's own non-blocking stream; to order work after the legacy default
+ * stream, pass cudaStreamLegacy). */
 DT_API int dt_ctx_set_stream(dt_ctx *ctx, void *stream);
 DT_API int dt_ctx_synchronize(dt_ctx *ctx);
 /* Message of the last failure on the calling thread ("" if none). */
@@ -186,6 +187,32 @@ DT_API int dt_ttm_tc(dt_ctx *ctx, const float *X, int ndim, const int64_t *shape
  * split-K partials).  The Gram of Function::gram (tensor.tpp:18-120) for
  * I <= 128, K % 8 == 0. */
 DT_API int dt_gram_tc(dt_ctx *ctx, const float *Y, int64_t I, int64_t K, int split, double *S);
+
+/* ---- learned warm start (no counterpart in the reference, which starts
+ * HOOI from random factors, hooi_als.tpp:74-81) -------------------------
+ * A linear autoencoder over factor columns of length n: encoder E (k x n),
+ * decoder D (n x k), both col-major FP64, k <= 32. */
+
+/* Loss |D E U - U|^2 / N over the N columns of U (n x N col-major) and its
+ * gradients dE (k x n), dD (n x k): one forward and backward pass. */
+DT_API int dt_ws_loss_grad(dt_ctx *ctx, const double *U, int64_t n, int64_t N, int k,
+                           const double *E, const double *D, double *loss, double *gE,
+                           double *gD);
+
+/* Trains E and D from seeded Gaussian weights with `steps` full-batch Adam
+ * steps (rate lr) on the columns of U; loss_hist (steps values, may be NULL)
+ * receives the loss before each step. */
+DT_API int dt_ws_train(dt_ctx *ctx, const double *U, int64_t n, int64_t N, int k, int steps,
+                       double lr, uint64_t seed, double *E, double *D, double *loss_hist);
+
+/* Initial factors for dense HOOI from the decoder D (n x k): sketch
+ * X x_m orth(D)^T over every mode (k^ndim values, one pass over X), leading
+ * R_m subspaces of the sketch refined by up to sketch_sweeps HOOI sweeps on
+ * the sketch, decoded to U[m] (n x R_m col-major).  Every mode has size n;
+ * R_m <= k.  fit_sketch = |sketch|^2 / |X|^2, fit_init = |X x_m U_m^T|^2 / |X|^2. */
+DT_API int dt_ws_init(dt_ctx *ctx, const void *X, int dtype, int ndim, const int64_t *shape,
+                      const int64_t *ranks, const double *D, int k, int sketch_sweeps,
+                      double *const *U, double *fit_sketch, double *fit_init);
 
 /* ---- dense HOOI ------------------------------------------------------- */
 /* Tucker decomposition of X (dtype DT_F64 or DT_F32, column-major) with the
