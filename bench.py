@@ -312,7 +312,7 @@ def run_ours(args):
         out["clocks"] = clk
     if args.ttmc and world == 1:
         _log("sparse TTMc")
-        out["ttmc"] = _ttmc(ctx, peak)
+        out["ttmc"] = _ttmc(ctx, peak, args.ttmc_draws)
     if args.warmstart and world == 1:
         _log("learned warm start")
         out["warmstart"] = _warmstart(ctx, args.ws_train, args.ws_eval)
@@ -328,13 +328,17 @@ def run_ours(args):
         print(json.dumps(out), flush=True)
 
 
-def _ttmc(ctx, peak):
+def _ttmc(ctx, peak, draws=50_000_000):
     """Sparse TTMc bandwidth on the 2,000,000 x 200,000 x 50,000 COO tensor
-    (50M Zipf(1.1) draws, merged), ranks 16^3: one sparse HOOI sweep with the
-    TTMc launches timed by CUDA events."""
+    (50M Zipf(1.1) draws, merged; fewer with --ttmc-draws), ranks 16^3: one
+    sparse HOOI sweep with the TTMc launches timed by CUDA events."""
     from diana_tucker_b200 import datasets
     t0 = time.time()
-    idx, vals, shape = datasets.sparse_2m_200k_50k()
+    if draws == 50_000_000:
+        idx, vals, shape = datasets.sparse_2m_200k_50k()
+    else:
+        idx, vals, shape = datasets.sparse_zipf((2_000_000, 200_000, 50_000), draws, alpha=1.1,
+                                                seed=2)
     gen_s = time.time() - t0
     sp = ctx.sptensor(idx, vals, shape)
     R = (16, 16, 16)
@@ -342,10 +346,16 @@ def _ttmc(ctx, peak):
     sp.hooi(R, 1, Ut)
     _, _, rep = sp.hooi(R, 1, Ut)
     gbs = rep["ttm_x_bytes"] / (rep["ttm_x_ms"] * 1e-3) / 1e9 if rep["ttm_x_ms"] else 0.0
+    # Every nonzero also gathers one row of each other factor (2 x 16 doubles):
+    # traffic the unblocked TTMc must move through L2 (and from HBM for the
+    # 2e6-row factor, which exceeds L2), outside the algorithmic bytes above.
+    gather = float(len(vals)) * 3 * (2 * 16 * 8)
+    eff = (rep["ttm_x_bytes"] + gather) / (rep["ttm_x_ms"] * 1e-3) / 1e9 if rep["ttm_x_ms"] else 0.0
     sp.close()
     return {"value": round(gbs, 1), "unit": "GB/s", "frac_of_hbm": round(gbs / peak, 4),
             "nnz": int(len(vals)), "launches": rep["ttm_x_launches"],
             "ms": rep["ttm_x_ms"], "bytes": rep["ttm_x_bytes"],
+            "gather_bytes": gather, "with_gathers_gbs": round(eff, 1),
             "sweep_ms": rep["device_ms"], "gen_s": round(gen_s, 1)}
 
 
@@ -436,6 +446,8 @@ def main(argv=None):
     ap.add_argument("--no-ttmc", dest="ttmc", action="store_false")
     ap.add_argument("--no-cpu", dest="cpu", action="store_false")
     ap.add_argument("--no-warmstart", dest="warmstart", action="store_false")
+    ap.add_argument("--ttmc-draws", type=int, default=50_000_000,
+                    help="Zipf draws of the sparse tensor (50M is the configured workload)")
     ap.add_argument("--ws-train", type=int, default=150,
                     help="warm-start training tensors (the full family split is 1500)")
     ap.add_argument("--ws-eval", type=int, default=50,

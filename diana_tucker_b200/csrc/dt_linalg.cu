@@ -1068,6 +1068,121 @@ __global__ void __launch_bounds__(256) rows_apply_kernel(const double *__restric
     }
 }
 
+// Row Gram on the FP64 tensor cores (mma.sync m8n8k4): A is r x m col-major
+// (factor row k = column k), G = sum_k a_k a_k^T.  With 4 columns per k-step,
+// the fragment A[g][t] = a_{4kk+t}(8h + g) is also the B fragment B[t][g] of
+// tile h, so each lane loads TT values per k-step for TT x TT MMAs.  Warps of
+// a block take interleaved k-steps of the block's column range; tiles are
+// summed over the warps in a fixed order into part[block][r*r].
+template <int RT>
+__global__ void __launch_bounds__(256) rows_gram_mma_kernel(const double *__restrict__ A, int r,
+                                                            int64_t m, int64_t cols_per_block,
+                                                            double *__restrict__ part) {
+    constexpr int TT = RT / 8;
+    __shared__ double red[4][RT * RT];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, g = lane >> 2, t = lane & 3;
+    const int64_t k0 = blockIdx.x * cols_per_block;
+    const int64_t k1 = min(m, k0 + cols_per_block);
+    double acc[TT][TT][2];
+#pragma unroll
+    for (int a = 0; a < TT; a++)
+#pragma unroll
+        for (int b = 0; b < TT; b++) acc[a][b][0] = acc[a][b][1] = 0.0;
+#pragma unroll 4
+    for (int64_t c0 = k0 + 4 * w; c0 < k1; c0 += 32) {
+        const int64_t col = c0 + t;
+        double f[TT];
+#pragma unroll
+        for (int h = 0; h < TT; h++)
+            f[h] = (col < k1 && 8 * h + g < r) ? A[col * r + 8 * h + g] : 0.0;
+#pragma unroll
+        for (int a = 0; a < TT; a++)
+#pragma unroll
+            for (int b = 0; b < TT; b++) {
+                asm volatile(
+                    "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                    : "+d"(acc[a][b][0]), "+d"(acc[a][b][1])
+                    : "d"(f[a]), "d"(f[b]));
+            }
+    }
+    // Warps 0-3 store, warps 4-7 add theirs (fixed order), then 4 slots sum.
+    if (w < 4) {
+#pragma unroll
+        for (int a = 0; a < TT; a++)
+#pragma unroll
+            for (int b = 0; b < TT; b++)
+#pragma unroll
+                for (int q = 0; q < 2; q++)
+                    red[w][(8 * a + g) * RT + 8 * b + 2 * t + q] = acc[a][b][q];
+    }
+    __syncthreads();
+    if (w >= 4) {
+#pragma unroll
+        for (int a = 0; a < TT; a++)
+#pragma unroll
+            for (int b = 0; b < TT; b++)
+#pragma unroll
+                for (int q = 0; q < 2; q++)
+                    red[w - 4][(8 * a + g) * RT + 8 * b + 2 * t + q] += acc[a][b][q];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < r * r; e += blockDim.x) {
+        const int i = e / r, j = e - i * r;
+        double s = 0.0;
+#pragma unroll
+        for (int q = 0; q < 4; q++) s += red[q][i * RT + j];
+        part[(int64_t)blockIdx.x * r * r + i * r + j] = s;
+    }
+}
+
+// T = Linv A on the FP64 tensor cores: Linv (r x r lower, col-major) is the A
+// operand (held in registers), 8-column blocks of A (r x m col-major) the B
+// operand; one warp per 8-column block.
+template <int RT>
+__global__ void __launch_bounds__(256) rows_apply_mma_kernel(const double *__restrict__ A, int r,
+                                                             int64_t m,
+                                                             const double *__restrict__ Linv,
+                                                             double *__restrict__ T) {
+    constexpr int TT = RT / 8, KS = RT / 4;
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    double la[TT][KS];
+#pragma unroll
+    for (int h = 0; h < TT; h++)
+#pragma unroll
+        for (int kk = 0; kk < KS; kk++) {
+            const int i = 8 * h + g, c = 4 * kk + t;
+            la[h][kk] = (i < r && c < r) ? Linv[i + (int64_t)r * c] : 0.0;
+        }
+    const int64_t warp0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int64_t nblk = (m + 7) / 8;
+    for (int64_t cb = warp0; cb < nblk; cb += nwarps) {
+        double acc[TT][2];
+#pragma unroll
+        for (int h = 0; h < TT; h++) acc[h][0] = acc[h][1] = 0.0;
+        const int64_t colb = 8 * cb + g;
+#pragma unroll
+        for (int kk = 0; kk < KS; kk++) {
+            const int c = 4 * kk + t;
+            const double b = (colb < m && c < r) ? A[colb * r + c] : 0.0;
+#pragma unroll
+            for (int h = 0; h < TT; h++)
+                asm volatile(
+                    "mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                    : "+d"(acc[h][0]), "+d"(acc[h][1])
+                    : "d"(la[h][kk]), "d"(b));
+        }
+#pragma unroll
+        for (int h = 0; h < TT; h++)
+#pragma unroll
+            for (int q = 0; q < 2; q++) {
+                const int64_t col = 8 * cb + 2 * t + q;
+                const int i = 8 * h + g;
+                if (col < m && i < r) T[col * r + i] = acc[h][q];
+            }
+    }
+}
+
 __global__ void sum_parts_kernel(const double *__restrict__ part, int nblk, int n,
                                  double *__restrict__ out) {
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
@@ -1236,15 +1351,28 @@ void orth2_rows(dt_ctx *ctx, double *A, int64_t len1, int64_t len2) {
         DevMem T(ctx, (size_t)r * len2 * sizeof(double));
         const unsigned ablocks = std::max(
             1u, std::min<unsigned>(ceil_div(len2 * r, 256), 16u * (unsigned)ctx->num_sms));
+        const int RT = r <= 8 ? 8 : (r <= 16 ? 16 : (r <= 24 ? 24 : 32));
+        const unsigned mblocks = (unsigned)std::max<int64_t>(
+            1, std::min<int64_t>(((len2 + 7) / 8 + 7) / 8, 8LL * ctx->num_sms));
         for (int pass = 0; pass < 2; pass++) {
             const double *src = pass == 0 ? A : T.as<double>();
             double *dst = pass == 0 ? T.as<double>() : A;
-            DT_LAUNCH(ctx, rows_gram_kernel, nblk, 256, 0, src, r, len2, rpb, part.as<double>());
-            DT_LAUNCH(ctx, sum_parts_kernel, 1, 256, 0, part.as<double>(), nblk, r * r,
-                      G.as<double>());
-            DT_LAUNCH(ctx, chol_lower_inv_kernel, 1, 256, 2 * r * r * sizeof(double),
-                      G.as<double>(), r, Li.as<double>(), flag.as<int>());
-            DT_LAUNCH(ctx, rows_apply_kernel, ablocks, 256, 0, src, r, len2, Li.as<double>(), dst);
+#define DT_ROWS(R)                                                                              \
+    do {                                                                                        \
+        DT_LAUNCH(ctx, rows_gram_mma_kernel<R>, nblk, 256, 0, src, r, len2, rpb,                \
+                  part.as<double>());                                                           \
+        DT_LAUNCH(ctx, sum_parts_kernel, 1, 256, 0, part.as<double>(), nblk, r * r,             \
+                  G.as<double>());                                                              \
+        DT_LAUNCH(ctx, chol_lower_inv_kernel, 1, 256, 2 * r * r * sizeof(double), G.as<double>(), \
+                  r, Li.as<double>(), flag.as<int>());                                          \
+        DT_LAUNCH(ctx, rows_apply_mma_kernel<R>, mblocks, 256, 0, src, r, len2, Li.as<double>(), \
+                  dst);                                                                         \
+    } while (0)
+            if (RT == 8) DT_ROWS(8);
+            else if (RT == 16) DT_ROWS(16);
+            else if (RT == 24) DT_ROWS(24);
+            else DT_ROWS(32);
+#undef DT_ROWS
         }
         int h = 0;
         DT_CUDA(cudaMemcpyAsync(&h, flag.get(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
