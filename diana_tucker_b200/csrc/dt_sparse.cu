@@ -4,12 +4,19 @@
 // ttmc_mTL (sp_tensor.tpp:236-365), and the sparse HOOI power sweep
 // (template/algorithm/sp_tucker/sp_hooi_als.tpp:48-118).
 //
-// TTMc work decomposition: the nonzeros of every non-empty mode-n row are cut
-// into chunks of at most CHUNK nonzeros; one warp owns one chunk and keeps the
-// row's P = prod_{m != n} R_m accumulators in registers (P/32 per lane).  A row
-// that fits one chunk is written directly; a longer row (Zipf-skewed heads)
-// writes per-chunk partial rows that a second kernel sums in chunk order.  The
-// output is therefore deterministic and needs no floating-point atomics.
+// 3-way tensors (the configured workload) use a fibre-factored layout.  For
+// mode n with other modes F (the "fibre" mode) and E, the nonzeros of row i_n
+// are grouped by i_F, and
+//     Y_(n)(i_n, :) = sum_{fibres f of the row} U_F(i_F(f), :) (x) w_f,
+//     w_f = sum_{nonzeros e of f} v_e U_E(i_E(e), :),
+// which costs R_E FMAs per nonzero and R_F R_E per fibre instead of R_F R_E per
+// nonzero.  The outer products run on the FP64 tensor cores (mma.sync m8n8k4):
+// four fibres form the K = 4 slice of one step.  Other orders use a row kernel
+// (one warp per chunk of a row).
+//
+// Long rows are cut into pieces that write partial rows; a second kernel sums
+// them in a fixed order, so the output is deterministic and needs no
+// floating-point atomics.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -24,15 +31,17 @@ namespace {
 
 constexpr int MAXD = 8;
 constexpr int64_t CHUNK = 512;
-constexpr int64_t TASK_PACK = 512;
-constexpr int64_t TASK_PIECE = 2048;
+constexpr int FIB_CHUNK = 8;
+constexpr int64_t TASK_PACK_GRP = 64;
+constexpr int64_t TASK_PIECE_GRP = 256;
 
 struct ModeCopy {
-    // Nonzeros sorted by this mode's index.
-    DevMem other;       // int32 [ndim-1][nnz]: the other modes' indices, in mode order
-    DevMem val;         // double [nnz]
     int64_t nrows = 0;  // non-empty rows
     DevMem rows;        // int32 [nrows]: row id of compact row k
+    // Row-kernel layout (orders other than 3): nonzeros sorted by this mode's
+    // index, cut into chunks of at most CHUNK nonzeros.
+    DevMem other;       // int32 [ndim-1][nnz]: the other modes' indices, in mode order
+    DevMem val;         // double [nnz]
     DevMem rowptr;      // int64 [nrows+1]
     int64_t nchunks = 0;
     DevMem chunk_row;   // int32 [nchunks]: compact row of the chunk
@@ -43,14 +52,24 @@ struct ModeCopy {
     DevMem multi_row;     // int32 [nmulti]: compact row
     DevMem multi_first;   // int32 [nmulti]: first partial slot
     DevMem multi_count;   // int32 [nmulti]
-    // Task list of the 3-way TTMc kernel: runs of whole consecutive rows with
-    // at most TASK_PACK nonzeros in all, and pieces of at most TASK_PIECE
-    // nonzeros of longer rows; sorted by size, largest first.
+    // Fibre layout (3-way): nonzeros ordered by (row, fibre); a row's fibres,
+    // cut into sub-fibres of at most FIB_CHUNK nonzeros, come longest first
+    // and are padded with empty fibres to a multiple of 4 (a group).
+    int fmode = -1;       // fibre mode F; the element mode E is the remaining one
+    int64_t nfib = 0;     // fibre slots (4 per group)
+    DevMem e_idx;         // int32 [nnz]: i_E of each nonzero, in fibre order
+    DevMem e_val;         // double [nnz]
+    DevMem fib_idx;       // int32 [nfib]: i_F of each fibre slot (0 when empty)
+    DevMem fib_ptr;       // int32 [nfib+1]: its nonzeros
+    DevMem grp_row;       // int32 [nfib/4 + 1]: compact row of each group, then -1
+    // Batches: int2 {first group, first nonzero} (+ an end entry); a batch is
+    // at most FB_GRP groups and FB_NZ nonzeros.  Tasks: int4 {first batch, end
+    // batch, partial slot or -1, 0}: packs of whole consecutive rows, or pieces
+    // of one long row, largest first.
+    int64_t nbatch = 0;
+    DevMem batches;
     int64_t ntasks = 0;
-    DevMem task_beg;      // int64 [ntasks]
-    DevMem task_end;      // int64 [ntasks]
-    DevMem task_row;      // int32 [ntasks]: compact row of the first nonzero
-    DevMem task_slot;     // int32 [ntasks]: -1 = rows written directly, else partial slot
+    DevMem tasks;
     int64_t tslots = 0;
     int64_t tmulti = 0;   // rows cut into several pieces
     DevMem tmulti_row, tmulti_first, tmulti_count;
@@ -105,12 +124,11 @@ __global__ void gather_kernel(const T *__restrict__ src, const int32_t *__restri
 }
 
 // ---------------------------------------------------------------------------
-// TTMc row kernel.  One warp per chunk.  Lane l owns Kronecker entries
-// p = l + 32 q (q < PL).  For 3-way tensors with R_a | 32 the entry p =
-// pa + R_a pb maps to a lane-constant pa, so each nonzero costs one factor-row
-// load per mode, PL shuffles and PL FMAs per lane.
+// TTMc row kernel (orders other than 3).  One warp per chunk.  Lane l owns
+// Kronecker entries p = l + 32 q (q < PL); per nonzero it multiplies the
+// value by the other factors' entries at its p.
 // ---------------------------------------------------------------------------
-template <int PL, bool FAST3>
+template <int PL>
 __global__ void __launch_bounds__(256) ttmc_rows_kernel(
     const int32_t *__restrict__ other, const double *__restrict__ val, int64_t nnz, int nother,
     const int64_t *__restrict__ rowptr, const int32_t *__restrict__ chunk_row,
@@ -119,11 +137,6 @@ __global__ void __launch_bounds__(256) ttmc_rows_kernel(
     const int lane = threadIdx.x & 31;
     const int64_t warp0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    // Per-lane Kronecker coordinates (FAST3: p = pa + Ra*pb).
-    const int Ra = f.R[0];
-    const int pa = FAST3 ? (lane % Ra) : 0;
-    const int pb0 = FAST3 ? (lane / Ra) : 0;
-    const int pbstep = FAST3 ? (32 / Ra) : 0;
     for (int64_t c = warp0; c < nchunks; c += nwarps) {
         const int32_t k = chunk_row[c];
         const int64_t beg = chunk_beg[c];
@@ -142,78 +155,99 @@ __global__ void __launch_bounds__(256) ttmc_rows_kernel(
             const int cnt = (int)(end - e0 < 32 ? end - e0 : 32);
             for (int j = 0; j < cnt; j++) {
                 const double v = __shfl_sync(0xffffffffu, myv, j);
-                if (FAST3) {
-                    const int ia = __shfl_sync(0xffffffffu, myidx[0], j);
-                    const int ib = __shfl_sync(0xffffffffu, myidx[1], j);
-                    const int Rb = f.R[1];
-                    const double ua = f.U[0][(int64_t)ia * Ra + pa];
-                    const double ubl = lane < Rb ? f.U[1][(int64_t)ib * Rb + lane] : 0.0;
-                    const double w = v * ua;
+                int32_t ix[MAXD - 1];
 #pragma unroll
-                    for (int q = 0; q < PL; q++) {
-                        const int pb = pb0 + q * pbstep;
-                        const double ub = __shfl_sync(0xffffffffu, ubl, pb & 31);
-                        acc[q] = fma(w, ub, acc[q]);
+                for (int d = 0; d < MAXD - 1; d++) ix[d] = __shfl_sync(0xffffffffu, myidx[d], j);
+#pragma unroll
+                for (int q = 0; q < PL; q++) {
+                    int p = lane + 32 * q;
+                    if (p >= P) break;
+                    double prod = v;
+                    for (int d = 0; d < nother; d++) {
+                        const int r = f.R[d];
+                        const int pd = p % r;
+                        p /= r;
+                        prod *= f.U[d][(int64_t)ix[d] * r + pd];
                     }
-                } else {
-                    int32_t ix[MAXD - 1];
-#pragma unroll
-                    for (int d = 0; d < MAXD - 1; d++)
-                        ix[d] = __shfl_sync(0xffffffffu, myidx[d], j);
-#pragma unroll
-                    for (int q = 0; q < PL; q++) {
-                        int p = lane + 32 * q;
-                        if (p >= P) break;
-                        double prod = v;
-                        for (int d = 0; d < nother; d++) {
-                            const int r = f.R[d];
-                            const int pd = p % r;
-                            p /= r;
-                            prod *= f.U[d][(int64_t)ix[d] * r + pd];
-                        }
-                        acc[q] += prod;
-                    }
+                    acc[q] += prod;
                 }
             }
         }
         const int32_t slot = chunk_slot[c];
         double *dst = slot < 0 ? Yc + (int64_t)k * P : Ypart + (int64_t)slot * P;
-        if (FAST3) {
 #pragma unroll
-            for (int q = 0; q < PL; q++) {
-                const int p = pa + Ra * (pb0 + q * pbstep);
-                if (p < P) dst[p] = acc[q];
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < PL; q++) {
-                const int p = lane + 32 * q;
-                if (p < P) dst[p] = acc[q];
-            }
+        for (int q = 0; q < PL; q++) {
+            const int p = lane + 32 * q;
+            if (p < P) dst[p] = acc[q];
         }
     }
 }
 
 // ---------------------------------------------------------------------------
-// 3-way TTMc over the task list (even ranks RA, RB of the two other modes; P =
-// RA * RB).  One warp per task.  Nonzeros go through in batches of 32:
-//  * lane j loads nonzero j's two indices and value (coalesced); the batch
-//    after next is already in registers, so these loads overlap compute;
-//  * the two factor rows of every nonzero (RA + RB doubles) are copied into a
-//    per-warp shared stage with 16-byte cp.async, double-buffered: batch b+1
-//    is in flight while batch b is consumed;
-//  * lane l owns BPL blocks of AW x BW Kronecker entries (p = pa + RA * pb);
-//    per nonzero it reads AW + BW staged values and v, then AW*BW FMAs;
-//  * a packed task walks whole rows: at each row boundary (from a register
-//    window of 32 rowptr entries) the warp writes its row and restarts.
-// Long rows arrive as pieces that write partial rows, summed in piece order by
-// combine_partials_kernel: the output is deterministic, without atomics.
+// FP64 tensor-core fragment helper (mma.sync m8n8k4 .f64).  Fragments: A[g][t]
+// and B[t][g] with g = lane / 4, t = lane % 4; the 8 x 8 result D[g][2t + {0,1}].
 // ---------------------------------------------------------------------------
-constexpr int T3_WARPS = 4;
+__device__ __forceinline__ void sp_dmma(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
 
-__device__ __forceinline__ void sp_cp_async16(void *smem, const void *gmem) {
+// ---------------------------------------------------------------------------
+// 3-way fibre TTMc.  The Kronecker index is p = p_lo + R_lo p_hi over the two
+// other modes (lower mode fastest, sp_tensor.tpp:367-417); the warp keeps the
+// current row as TR x TC tiles of 8 x 8 with rows = p_hi and columns = p_lo,
+// so each lane's two accumulators of a tile are adjacent in memory.
+//
+// Layout: every row's (sub-)fibres, longest first, padded to a multiple of 4
+// with empty fibres; four consecutive fibres form a group, the K = 4 slice of
+// one mma.sync step.  Lane (g, t) takes fibre t of the group: it sums
+// w = sum_e v_e U_E(i_E(e), g + 8 j) over its fibre's nonzeros and reads
+// U_F(i_F, g + 8 j) -- exactly its A / B fragment elements -- so the group's
+// four outer products are TF x TE mma.sync steps with no redundant FMAs.
+// FLO: the fibre mode is the lower of the two (columns are p_F), else the
+// higher (rows are p_F).
+//
+// Pipeline (one warp per task = a run of batches; a batch is at most FB_GRP
+// groups and FB_NZ nonzeros, precomputed):
+//  * batch b + 2: fibre indices / offsets, nonzero indices / values and the
+//    groups' rows are loaded into registers (coalesced, one lane per item);
+//  * batch b + 1: its U_E rows (one per nonzero) and U_F rows (one per fibre)
+//    are copied by 16-byte cp.async into the warp's shared stage (the values
+//    and offsets by plain stores);
+//  * batch b: the fibre sums and the mma.sync steps read only shared memory.
+// A row is written when its last group is done (rows of a task are whole,
+// except pieces of long rows, which write a partial row at the task's end).
+// ---------------------------------------------------------------------------
+constexpr int FB_NZ = 32;
+constexpr int FB_GRP = 4;
+constexpr int FB_SLOTS = 4 * FB_GRP;
+
+// Shared row pitch (doubles) for a staged factor row of R entries: even (16-byte
+// pieces) and 4 mod 8, so four rows read by one fragment load start in
+// different banks.
+__host__ __device__ constexpr int fb_pitch(int R) {
+    int p = (R + 1) & ~1;
+    while (p % 8 != 4) p += 2;
+    return p;
+}
+
+template <int TF, int TE>
+struct FbStage {
+    static constexpr int PE = fb_pitch(8 * TE), PF = fb_pitch(8 * TF);
+    static constexpr int DOUBLES = FB_NZ * PE + FB_SLOTS * PF + FB_NZ;
+    static constexpr int INTS = FB_SLOTS + 1 + FB_GRP + 1;
+    static constexpr int BYTES = DOUBLES * 8 + ((INTS * 4 + 15) & ~15);
+    static constexpr int WARP_BYTES = 2 * BYTES;
+};
+
+__device__ __forceinline__ void sp_cp16(void *smem, const void *gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void sp_cp8(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void sp_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
@@ -221,204 +255,310 @@ __device__ __forceinline__ void sp_cp_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-template <int RA, int RB, int AW, int BW>
-struct T3 {
-    static constexpr int P = RA * RB;
-    static constexpr int NBA = RA / AW, NBB = RB / BW, NBLK = NBA * NBB;
-    static constexpr int BPL = (NBLK + 31) / 32;
-    static constexpr int ROWW = RA + RB;  // staged doubles per nonzero
-    static constexpr int PPN = ROWW / 2;  // 16-byte pieces per nonzero
-    static constexpr int STAGE = 32 * ROWW;
-    static constexpr int WARP_SMEM = 2 * STAGE + 32;  // doubles per warp
+struct FbMeta {
+    int g0, ng, nz0, nzn;
+    int fidx, fofs, grow;
+    int idx;
+    double v;
 };
 
-template <int RA, int RB, int AW, int BW>
-__global__ void __launch_bounds__(T3_WARPS * 32) ttmc3_kernel(
-    const int32_t *__restrict__ ia_arr, const int32_t *__restrict__ ib_arr,
-    const double *__restrict__ val, const int64_t *__restrict__ rowptr, int64_t nrows,
-    const int64_t *__restrict__ task_beg, const int64_t *__restrict__ task_end,
-    const int32_t *__restrict__ task_row, const int32_t *__restrict__ task_slot, int64_t ntasks,
-    const double *__restrict__ Ua, const double *__restrict__ Ub, double *__restrict__ Yc,
-    double *__restrict__ Ypart) {
-    using C = T3<RA, RB, AW, BW>;
-    static_assert(RA % 2 == 0 && RB % 2 == 0 && RA % AW == 0 && RB % BW == 0, "tile shape");
-    static_assert(AW == 1 || AW == 2, "AW");
-    static_assert(BW == 2 || BW == 4, "BW");
-    extern __shared__ __align__(16) double t3_smem[];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    double *stage0 = t3_smem + (size_t)wib * C::WARP_SMEM;
-    double *vbuf = stage0 + 2 * C::STAGE;
-    const int64_t gw = (int64_t)blockIdx.x * T3_WARPS + wib;
-    const int64_t nw = (int64_t)gridDim.x * T3_WARPS;
+// Registers of batch b: lane l holds fibre slot l (index, offset into the
+// batch's nonzeros), nonzero l (index, value) and the row of group l (l <= ng;
+// the entry after the batch tells whether its last group ends a row).
+__device__ __forceinline__ void fb_load_meta(FbMeta &m, int b, int lane,
+                                             const int2 *__restrict__ bt,
+                                             const int32_t *__restrict__ grp_row,
+                                             const int32_t *__restrict__ fib_idx,
+                                             const int32_t *__restrict__ fib_ptr,
+                                             const int32_t *__restrict__ e_idx,
+                                             const double *__restrict__ e_val) {
+    const int2 c = bt[b], d = bt[b + 1];
+    m.g0 = c.x;
+    m.ng = d.x - c.x;
+    m.nz0 = c.y;
+    m.nzn = d.y - c.y;
+    const bool sv = lane < 4 * m.ng;
+    m.fidx = sv ? fib_idx[4 * m.g0 + lane] : 0;
+    m.fofs = sv ? fib_ptr[4 * m.g0 + lane] - m.nz0 : 0;
+    m.grow = lane <= m.ng ? grp_row[m.g0 + lane] : -1;
+    const bool a = lane < m.nzn;
+    m.idx = a ? e_idx[m.nz0 + lane] : 0;
+    m.v = a ? e_val[m.nz0 + lane] : 0.0;
+}
 
-    // Lane-owned blocks.
-    int oa[C::BPL], ob[C::BPL];
-    bool own[C::BPL];
-#pragma unroll
-    for (int q = 0; q < C::BPL; q++) {
-        const int blk = lane + 32 * q;
-        own[q] = blk < C::NBLK;
-        oa[q] = own[q] ? AW * (blk % C::NBA) : 0;
-        ob[q] = own[q] ? BW * (blk / C::NBA) : 0;
+__host__ __device__ constexpr int fb_pow2(int x) {
+    int p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+
+// Copies n <= 32 rows of the transposed factor U (R <= RMAX doubles each; the
+// index of row j is held by lane j) into dst rows of `pitch` doubles.  Lane l
+// copies piece l % PPR of row l / PPR (+ 32 / PPR per step), PPR a power of
+// two: 16-byte pieces when R is even and U 16-byte aligned, else 8-byte ones.
+template <int RMAX>
+__device__ __forceinline__ void fb_stage_rows(double *dst, int pitch, const double *__restrict__ U,
+                                              int R, int n, int ridx, int lane) {
+    if ((R & 1) == 0 && (reinterpret_cast<uintptr_t>(U) & 15) == 0) {
+        constexpr int PPR = fb_pow2(RMAX / 2), RPI = 32 / PPR;
+        const int rem = lane % PPR, jl = lane / PPR;
+        const bool okp = 2 * rem < R;
+        for (int j0 = 0; j0 < n; j0 += RPI) {
+            const int j = j0 + jl;
+            const int i = __shfl_sync(0xffffffffu, ridx, j & 31);
+            if (j < n && okp) sp_cp16(dst + j * pitch + 2 * rem, U + (int64_t)i * R + 2 * rem);
+        }
+    } else {
+        constexpr int PPR = fb_pow2(RMAX), RPI = 32 / PPR;
+        const int rem = lane % PPR, jl = lane / PPR;
+        const bool okp = rem < R;
+        for (int j0 = 0; j0 < n; j0 += RPI) {
+            const int j = j0 + jl;
+            const int i = __shfl_sync(0xffffffffu, ridx, j & 31);
+            if (j < n && okp) sp_cp8(dst + j * pitch + rem, U + (int64_t)i * R + rem);
+        }
     }
+}
 
-    for (int64_t t = gw; t < ntasks; t += nw) {
-        const int64_t beg = task_beg[t], end = task_end[t];
-        int64_t row = task_row[t];
-        const int32_t slot = task_slot[t];
-        const int nb = (int)((end - beg + 31) / 32);
+template <int TF, int TE, bool FLO>
+__global__ void __launch_bounds__(256, 2) ttmc3f_kernel(
+    const int4 *__restrict__ tasks, int64_t ntasks, const int2 *__restrict__ bt,
+    const int32_t *__restrict__ grp_row, const int32_t *__restrict__ fib_idx,
+    const int32_t *__restrict__ fib_ptr, const int32_t *__restrict__ e_idx,
+    const double *__restrict__ e_val, const double *__restrict__ UF, int RF,
+    const double *__restrict__ UE, int RE, double *__restrict__ Yc, double *__restrict__ Ypart,
+    int *__restrict__ next_task) {
+    using S = FbStage<TF, TE>;
+    constexpr int TR = FLO ? TE : TF, TC = FLO ? TF : TE;
+    extern __shared__ __align__(16) unsigned char fb_smem[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, g = lane >> 2, t4 = lane & 3;
+    const int nwarp_blk = blockDim.x >> 5;
+    unsigned char *wsm = fb_smem + (size_t)wib * S::WARP_BYTES;
+    const int64_t gw = (int64_t)blockIdx.x * nwarp_blk + wib;
+    const int64_t nw = (int64_t)gridDim.x * nwarp_blk;
+    const int P = RF * RE;
+    const int Rlo = FLO ? RF : RE, Rhi = FLO ? RE : RF;
+    const int pe = fb_pitch(RE), pf = fb_pitch(RF);
+    bool okF[TF], okE[TE];
+#pragma unroll
+    for (int j = 0; j < TF; j++) okF[j] = g + 8 * j < RF;
+#pragma unroll
+    for (int j = 0; j < TE; j++) okE[j] = g + 8 * j < RE;
 
-        // Row-boundary window: lane l holds rowptr[wbase + 1 + l].
-        int64_t wbase = row;
-        int64_t bnd_win = (wbase + 1 + lane <= nrows) ? rowptr[wbase + 1 + lane] : INT64_MAX;
-        int wi = 0;
+    auto ue_of = [&](int buf) { return reinterpret_cast<double *>(wsm + buf * S::BYTES); };
+    auto uf_of = [&](int buf) { return ue_of(buf) + FB_NZ * S::PE; };
+    auto vv_of = [&](int buf) { return uf_of(buf) + FB_SLOTS * S::PF; };
+    auto fo_of = [&](int buf) {
+        return reinterpret_cast<int *>(wsm + buf * S::BYTES + S::DOUBLES * 8);
+    };
 
-        auto load_idx = [&](int b, int &ia, int &ib, double &v) {
-            const int64_t e = beg + 32 * (int64_t)b + lane;
-            const bool ok = e < end;
-            ia = ok ? ia_arr[e] : 0;
-            ib = ok ? ib_arr[e] : 0;
-            v = ok ? val[e] : 0.0;
-        };
-        auto issue = [&](int b, int ia, int ib) {
-            double *st = stage0 + (b & 1) * C::STAGE;
-            const int64_t e0 = beg + 32 * (int64_t)b;
-            const int n_b = (int)(end - e0 < 32 ? end - e0 : 32);
-#pragma unroll
-            for (int s = 0; s < C::PPN; s++) {
-                const int g = lane + 32 * s;
-                const int jj = g / C::PPN, rem = g - jj * C::PPN;
-                const int ija = __shfl_sync(0xffffffffu, ia, jj);
-                const int ijb = __shfl_sync(0xffffffffu, ib, jj);
-                if (jj < n_b) {
-                    const double *src = rem < RA / 2 ? Ua + (int64_t)ija * RA + 2 * rem
-                                                     : Ub + (int64_t)ijb * RB + 2 * (rem - RA / 2);
-                    sp_cp_async16(st + jj * C::ROWW + 2 * rem, src);
-                }
-            }
-            sp_cp_commit();
-        };
+    auto stage = [&](const FbMeta &m, int buf) {
+        double *vv = vv_of(buf);
+        int *fo = fo_of(buf);
+        int *gr = fo + FB_SLOTS + 1;
+        vv[lane] = m.v;
+        if (lane < 4 * m.ng) fo[lane] = m.fofs;
+        if (lane == 0) fo[4 * m.ng] = m.nzn;
+        if (lane <= m.ng) gr[lane] = m.grow;
+        fb_stage_rows<8 * TE>(ue_of(buf), pe, UE, RE, m.nzn, m.idx, lane);
+        fb_stage_rows<8 * TF>(uf_of(buf), pf, UF, RF, 4 * m.ng, m.fidx, lane);
+        sp_cp_commit();
+    };
 
-        double acc[C::BPL][AW][BW];
+    double acc[TR][TC][2];
 #pragma unroll
-        for (int q = 0; q < C::BPL; q++)
+    for (int r = 0; r < TR; r++)
 #pragma unroll
-            for (int u = 0; u < AW; u++)
-#pragma unroll
-                for (int w = 0; w < BW; w++) acc[q][u][w] = 0.0;
+        for (int c = 0; c < TC; c++) acc[r][c][0] = acc[r][c][1] = 0.0;
 
-        auto flush = [&](int64_t r) {
-            double *dst = slot < 0 ? Yc + r * C::P : Ypart + (int64_t)slot * C::P;
-#pragma unroll
-            for (int q = 0; q < C::BPL; q++) {
-                if (!own[q]) continue;
-#pragma unroll
-                for (int w = 0; w < BW; w++) {
-                    double *d = dst + oa[q] + RA * (ob[q] + w);
-                    if (AW == 2)
-                        *reinterpret_cast<double2 *>(d) = make_double2(acc[q][0][w], acc[q][AW - 1][w]);
-                    else
-                        d[0] = acc[q][0][w];
-#pragma unroll
-                    for (int u = 0; u < AW; u++) acc[q][u][w] = 0.0;
-                }
-            }
-        };
-
-        int a_ia, a_ib;
-        double a_v, cur_v, nxt_v = 0.0;
-        load_idx(0, a_ia, a_ib, a_v);
-        issue(0, a_ia, a_ib);
-        cur_v = a_v;
-        if (nb > 1) load_idx(1, a_ia, a_ib, a_v);
-        int64_t next_bnd = __shfl_sync(0xffffffffu, bnd_win, 0);
-
-        for (int b = 0; b < nb; b++) {
-            if (b + 1 < nb) {
-                issue(b + 1, a_ia, a_ib);
-                nxt_v = a_v;
-                if (b + 2 < nb) load_idx(b + 2, a_ia, a_ib, a_v);
+    // The first task of each warp is its own; later ones come from a counter
+    // (dynamic balance over the largest-first task list).
+    for (int64_t tk = gw; tk < ntasks;) {
+        const int4 task = tasks[tk];
+        const int b0 = task.x, b1 = task.y, slot = task.z;
+        FbMeta m;
+        fb_load_meta(m, b0, lane, bt, grp_row, fib_idx, fib_ptr, e_idx, e_val);
+        stage(m, 0);
+        int ng_cur = m.ng, ng_next = 0;
+        if (b0 + 1 < b1) fb_load_meta(m, b0 + 1, lane, bt, grp_row, fib_idx, fib_ptr, e_idx, e_val);
+        for (int b = b0; b < b1; b++) {
+            const int buf = (b - b0) & 1;
+            if (b + 1 < b1) {
+                stage(m, buf ^ 1);
+                ng_next = m.ng;
+                if (b + 2 < b1)
+                    fb_load_meta(m, b + 2, lane, bt, grp_row, fib_idx, fib_ptr, e_idx, e_val);
                 sp_cp_wait<1>();
             } else {
                 sp_cp_wait<0>();
             }
-            vbuf[lane] = cur_v;
             __syncwarp();
-            const double *st = stage0 + (b & 1) * C::STAGE;
-            const int64_t e0 = beg + 32 * (int64_t)b;
-            const int n_b = (int)(end - e0 < 32 ? end - e0 : 32);
-            for (int j = 0; j < n_b; j++) {
-                if (e0 + j == next_bnd) {
-                    flush(row);
-                    row++;
-                    if (++wi == 32) {
-                        wbase += 32;
-                        wi = 0;
-                        bnd_win = (wbase + 1 + lane <= nrows) ? rowptr[wbase + 1 + lane] : INT64_MAX;
+            const double *ue = ue_of(buf), *uf = uf_of(buf), *vv = vv_of(buf);
+            const int *fo = fo_of(buf);
+            const int *gr = fo + FB_SLOTS + 1;
+            for (int j = 0; j < ng_cur; j++) {
+                const int s = 4 * j + t4;
+                const int beg = fo[s], len = fo[s + 1] - beg;
+                int mx = max(len, __shfl_xor_sync(0xffffffffu, len, 1));
+                mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
+                double w[TE];
+#pragma unroll
+                for (int k = 0; k < TE; k++) w[k] = 0.0;
+                for (int q = 0; q < mx; q++) {
+                    if (q < len) {
+                        const double v = vv[beg + q];
+                        const double *row = ue + (beg + q) * pe + g;
+#pragma unroll
+                        for (int k = 0; k < TE; k++)
+                            if (okE[k]) w[k] = fma(v, row[8 * k], w[k]);
                     }
-                    next_bnd = __shfl_sync(0xffffffffu, bnd_win, wi);
                 }
-                const double v = vbuf[j];
-                const double *srow = st + j * C::ROWW;
+                double u[TF];
 #pragma unroll
-                for (int q = 0; q < C::BPL; q++) {
-                    if (!own[q]) continue;
-                    double wa[AW], ub[BW];
-                    if (AW == 2) {
-                        const double2 x = *reinterpret_cast<const double2 *>(srow + oa[q]);
-                        wa[0] = v * x.x;
-                        wa[AW - 1] = v * x.y;
-                    } else {
-                        wa[0] = v * srow[oa[q]];
+                for (int k = 0; k < TF; k++) u[k] = (okF[k] && len > 0) ? uf[s * pf + g + 8 * k] : 0.0;
+#pragma unroll
+                for (int r = 0; r < TR; r++)
+#pragma unroll
+                    for (int c = 0; c < TC; c++)
+                        sp_dmma(acc[r][c][0], acc[r][c][1], FLO ? w[r] : u[r], FLO ? u[c] : w[c]);
+                const int row = gr[j];
+                if (gr[j + 1] != row || (b == b1 - 1 && j == ng_cur - 1)) {
+                    double *dst = slot >= 0 ? Ypart + (int64_t)slot * P : Yc + (int64_t)row * P;
+#pragma unroll
+                    for (int r = 0; r < TR; r++) {
+                        const int ph = 8 * r + g;
+#pragma unroll
+                        for (int c = 0; c < TC; c++) {
+                            const int pl = 8 * c + 2 * t4;
+                            if (ph < Rhi) {
+                                double *d = dst + pl + (int64_t)Rlo * ph;
+                                if ((Rlo & 1) == 0 && pl + 1 < Rlo) {
+                                    *reinterpret_cast<double2 *>(d) =
+                                        make_double2(acc[r][c][0], acc[r][c][1]);
+                                } else {
+                                    if (pl < Rlo) d[0] = acc[r][c][0];
+                                    if (pl + 1 < Rlo) d[1] = acc[r][c][1];
+                                }
+                            }
+                            acc[r][c][0] = acc[r][c][1] = 0.0;
+                        }
                     }
-#pragma unroll
-                    for (int w = 0; w < BW; w += 2) {
-                        const double2 y = *reinterpret_cast<const double2 *>(srow + RA + ob[q] + w);
-                        ub[w] = y.x;
-                        ub[w + 1] = y.y;
-                    }
-#pragma unroll
-                    for (int u = 0; u < AW; u++)
-#pragma unroll
-                        for (int w = 0; w < BW; w++) acc[q][u][w] = fma(wa[u], ub[w], acc[q][u][w]);
                 }
             }
-            cur_v = nxt_v;
             __syncwarp();
+            ng_cur = ng_next;
         }
-        flush(row);
+        int nt = 0;
+        if (lane == 0) nt = atomicAdd(next_task, 1);
+        tk = nw + __shfl_sync(0xffffffffu, nt, 0);
     }
 }
 
-// Yc[row] = sum of its partial rows, in chunk order (deterministic).
-__global__ void combine_partials_kernel(const double *__restrict__ Ypart,
-                                        const int32_t *__restrict__ multi_row,
-                                        const int32_t *__restrict__ multi_first,
-                                        const int32_t *__restrict__ multi_count, int64_t nmulti,
-                                        int P, double *__restrict__ Yc) {
+// Fibre TTMc for other-mode ranks above 32 (P <= 1024): lane l owns Kronecker
+// entries p = l + 32 q, q < PL; per fibre it accumulates w at its p_E, then
+// one FMA with U_F at its p_F.  Same task / batch / group structure.
+template <int PL, bool FLO>
+__global__ void __launch_bounds__(256) ttmc3f_wide_kernel(
+    const int4 *__restrict__ tasks, int64_t ntasks, const int2 *__restrict__ bt,
+    const int32_t *__restrict__ grp_row, const int32_t *__restrict__ fib_idx,
+    const int32_t *__restrict__ fib_ptr, const int32_t *__restrict__ e_idx,
+    const double *__restrict__ e_val, const double *__restrict__ UF, int RF,
+    const double *__restrict__ UE, int RE, double *__restrict__ Yc, double *__restrict__ Ypart) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int P = RF * RE;
+    const int Rlo = FLO ? RF : RE;
+    int pF[PL], pE[PL];
+#pragma unroll
+    for (int q = 0; q < PL; q++) {
+        const int p = min(lane + 32 * q, P - 1);
+        const int lo = p % Rlo, hi = p / Rlo;
+        pF[q] = FLO ? lo : hi;
+        pE[q] = FLO ? hi : lo;
+    }
+    double acc[PL];
+#pragma unroll
+    for (int q = 0; q < PL; q++) acc[q] = 0.0;
+    for (int64_t tk = gw; tk < ntasks; tk += nw) {
+        const int4 task = tasks[tk];
+        const int gbeg = bt[task.x].x, gend = bt[task.y].x, slot = task.z;
+        for (int gq = gbeg; gq < gend; gq++) {
+            for (int f = 4 * gq; f < 4 * gq + 4; f++) {
+                const int fi = fib_idx[f], b = fib_ptr[f], e = fib_ptr[f + 1];
+                if (b == e) continue;
+                double w[PL];
+#pragma unroll
+                for (int q = 0; q < PL; q++) w[q] = 0.0;
+                for (int j = b; j < e; j++) {
+                    const double v = __ldg(e_val + j);
+                    const double *u = UE + (int64_t)__ldg(e_idx + j) * RE;
+#pragma unroll
+                    for (int q = 0; q < PL; q++) w[q] = fma(v, __ldg(u + pE[q]), w[q]);
+                }
+                const double *u = UF + (int64_t)fi * RF;
+#pragma unroll
+                for (int q = 0; q < PL; q++) acc[q] = fma(__ldg(u + pF[q]), w[q], acc[q]);
+            }
+            const int row = grp_row[gq];
+            if (grp_row[gq + 1] != row || gq == gend - 1) {
+                double *dst = slot >= 0 ? Ypart + (int64_t)slot * P : Yc + (int64_t)row * P;
+#pragma unroll
+                for (int q = 0; q < PL; q++) {
+                    if (lane + 32 * q < P) dst[lane + 32 * q] = acc[q];
+                    acc[q] = 0.0;
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Yc[row] = sum of its partial rows.  One CTA of 4 x 256 threads per row:
+// thread (s, x) sums partials c = s, s + 4, ... of entry p = x (+ 256 ...)
+// into four accumulators (c mod 16), so 16 independent loads are in flight;
+// the 4 x 4 accumulators are then added in a fixed order (deterministic).
+// ---------------------------------------------------------------------------
+constexpr int COMB_SPLIT = 4;
+__global__ void __launch_bounds__(1024) combine_partials_kernel(
+    const double *__restrict__ Ypart, const int32_t *__restrict__ multi_row,
+    const int32_t *__restrict__ multi_first, const int32_t *__restrict__ multi_count,
+    int64_t nmulti, int P, double *__restrict__ Yc) {
+    __shared__ double red[COMB_SPLIT][256];
+    const int s = threadIdx.x >> 8, x = threadIdx.x & 255;
     for (int64_t m = blockIdx.x; m < nmulti; m += gridDim.x) {
         const int32_t k = multi_row[m];
         const int64_t first = multi_first[m];
         const int cnt = multi_count[m];
-        for (int p = threadIdx.x; p < P; p += blockDim.x) {
-            double s = 0.0;
-            for (int c = 0; c < cnt; c++) s += Ypart[(first + c) * P + p];
-            Yc[(int64_t)k * P + p] = s;
+        for (int p0 = 0; p0 < P; p0 += 256) {
+            const int p = p0 + x;
+            double a[4] = {0.0, 0.0, 0.0, 0.0};
+            if (p < P) {
+                const double *src = Ypart + (first + s) * P + p;
+                int c = s;
+                for (; c + 3 * COMB_SPLIT < cnt; c += 4 * COMB_SPLIT) {
+#pragma unroll
+                    for (int j = 0; j < 4; j++) a[j] += src[(int64_t)j * COMB_SPLIT * P];
+                    src += (int64_t)4 * COMB_SPLIT * P;
+                }
+#pragma unroll
+                for (int j = 0; j < 3; j++)
+                    if (c + j * COMB_SPLIT < cnt) a[j] += src[(int64_t)j * COMB_SPLIT * P];
+            }
+            red[s][x] = (a[0] + a[1]) + (a[2] + a[3]);
+            __syncthreads();
+            if (s == 0 && p < P)
+                Yc[(int64_t)k * P + p] = (red[0][x] + red[1][x]) + (red[2][x] + red[3][x]);
+            __syncthreads();
         }
     }
 }
 
 // ---------------------------------------------------------------------------
-// ttmc_mTL / ttmc_mTR on the FP64 tensor-core path (mma.sync m8n8k4 .f64).
-// Operand fragments: A[g][t] and B[t][g] with g = lane / 4, t = lane % 4;
-// the 8 x 8 result D[g][2t + {0, 1}].  Staged shared operands use a pitch of
-// 4 (mod 16) doubles so a half-warp's fragment loads hit distinct banks.
+// ttmc_mTL / ttmc_mTR on the FP64 tensor-core path (sp_dmma above).  Staged
+// shared operands use a pitch of 4 (mod 16) doubles so a half-warp's fragment
+// loads hit distinct banks.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void sp_dmma(double &d0, double &d1, double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
-                 : "+d"(d0), "+d"(d1)
-                 : "d"(a), "d"(b));
-}
 
 // out[rows[k] * Rn + r] = sum_p Yc[k, p] L[p + P r].  One warp per 8 compact
 // rows; NTL = ceil(Rn / 8) output tiles.  L staged in shared memory (pitch
@@ -570,18 +710,34 @@ int64_t kron_len(const int64_t *R, int ndim, int mode) {
     return P;
 }
 
-void build_mode(dt_ctx *ctx, dt_sptensor *sp, int n, const std::vector<DevMem> &idx32,
-                const double *vals_dev) {
+// Uploads a host vector into a device buffer (at least 8 bytes).
+template <class T>
+void upload(dt_ctx *ctx, DevMem &dst, const std::vector<T> &src) {
+    const size_t bytes = src.size() * sizeof(T);
+    dst.alloc(ctx, std::max<size_t>(bytes, 8));
+    if (bytes)
+        DT_CUDA(cudaMemcpyAsync(dst.get(), src.data(), bytes, cudaMemcpyHostToDevice,
+                                ctx->stream));
+}
+
+int index_bits(int64_t extent) {
+    int bits = 1;
+    while ((int64_t(1) << bits) < extent) bits++;
+    return bits;
+}
+
+// Row-kernel layout: stable radix sort of (row index, nonzero id), the other
+// modes' indices and the values gathered into that order, and the chunk list.
+void build_mode_rows(dt_ctx *ctx, dt_sptensor *sp, int n, const std::vector<DevMem> &idx32,
+                     const double *vals_dev) {
     ModeCopy &mc = sp->modes[n];
     const int64_t nnz = sp->nnz;
     const int nd = sp->ndim;
     const unsigned blocks = std::max(1u, std::min<unsigned>(ceil_div(nnz, 256), 8 * ctx->num_sms));
-    // Stable radix sort of (row index, nonzero id).
     DevMem ids(ctx, nnz * sizeof(int32_t)), keys_out(ctx, nnz * sizeof(int32_t)),
         perm(ctx, nnz * sizeof(int32_t));
     DT_LAUNCH(ctx, iota_kernel, blocks, 256, 0, ids.as<int32_t>(), nnz);
-    int bits = 1;
-    while ((int64_t(1) << bits) < sp->shape[n]) bits++;
+    const int bits = index_bits(sp->shape[n]);
     size_t tmp_bytes = 0;
     DT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, idx32[n].as<int32_t>(),
                                             keys_out.as<int32_t>(), ids.as<int32_t>(),
@@ -638,131 +794,304 @@ void build_mode(dt_ctx *ctx, dt_sptensor *sp, int n, const std::vector<DevMem> &
     mc.nchunks = (int64_t)crow.size();
     mc.nslots = slots;
     mc.nmulti = (int64_t)mrow.size();
-    // Tasks of the 3-way kernel.
+    upload(ctx, mc.rows, rows);
+    upload(ctx, mc.rowptr, rowptr);
+    upload(ctx, mc.chunk_row, crow);
+    upload(ctx, mc.chunk_beg, cbeg);
+    upload(ctx, mc.chunk_slot, cslot);
+    upload(ctx, mc.multi_row, mrow);
+    upload(ctx, mc.multi_first, mfirst);
+    upload(ctx, mc.multi_count, mcount);
+    DT_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+__global__ void fibre_key_kernel(const int32_t *__restrict__ in, const int32_t *__restrict__ iF,
+                                 int bitsF, int64_t n, uint64_t *__restrict__ key) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
+         e += (int64_t)gridDim.x * blockDim.x)
+        key[e] = ((uint64_t)(uint32_t)in[e] << bitsF) | (uint32_t)iF[e];
+}
+
+// Fibre layout of a 3-way tensor for mode n.  Both other modes are tried as
+// the fibre mode F (radix sort of the 64-bit key (i_n, i_F) with the nonzero
+// ids); the one giving fewer fibres is kept.  On the host: fibres longer than
+// FIB_CHUNK nonzeros are cut into sub-fibres, a row's (sub-)fibres are ordered
+// by length, longest first (stable), and the nonzeros are permuted to follow;
+// the task list packs whole rows and cuts long rows into pieces.
+void build_mode_fibre(dt_ctx *ctx, dt_sptensor *sp, int n, const std::vector<DevMem> &idx32,
+                      const double *vals_dev) {
+    ModeCopy &mc = sp->modes[n];
+    const int64_t nnz = sp->nnz;
+    int oth[2], d = 0;
+    for (int m = 0; m < 3; m++)
+        if (m != n) oth[d++] = m;
+    const unsigned blocks = std::max(1u, std::min<unsigned>(ceil_div(nnz, 256), 8 * ctx->num_sms));
+    const int bits_n = index_bits(sp->shape[n]);
+    DevMem key(ctx, nnz * sizeof(uint64_t)), key_s(ctx, nnz * sizeof(uint64_t)),
+        ids(ctx, nnz * sizeof(int32_t)), ids_s(ctx, nnz * sizeof(int32_t));
+    std::vector<uint64_t> hkey((size_t)nnz), best_key;
+    std::vector<int32_t> best_ids((size_t)nnz);
+    int64_t best_fib = -1;
+    int best_F = -1, best_bits = 0;
+    DevMem tmp;
+    size_t tmp_have = 0;
+    for (int c = 0; c < 2; c++) {
+        const int F = oth[c];
+        const int bits_F = index_bits(sp->shape[F]);
+        DT_LAUNCH(ctx, fibre_key_kernel, blocks, 256, 0, idx32[n].as<int32_t>(),
+                  idx32[F].as<int32_t>(), bits_F, nnz, key.as<uint64_t>());
+        DT_LAUNCH(ctx, iota_kernel, blocks, 256, 0, ids.as<int32_t>(), nnz);
+        size_t tmp_bytes = 0;
+        DT_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, key.as<uint64_t>(),
+                                                key_s.as<uint64_t>(), ids.as<int32_t>(),
+                                                ids_s.as<int32_t>(), (int)nnz, 0,
+                                                bits_n + bits_F, ctx->stream));
+        if (tmp_bytes > tmp_have) {
+            tmp.alloc(ctx, tmp_bytes);
+            tmp_have = tmp_bytes;
+        }
+        DT_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tmp_bytes, key.as<uint64_t>(),
+                                                key_s.as<uint64_t>(), ids.as<int32_t>(),
+                                                ids_s.as<int32_t>(), (int)nnz, 0,
+                                                bits_n + bits_F, ctx->stream));
+        ctx->launches += 1;
+        DT_CUDA(cudaMemcpyAsync(hkey.data(), key_s.get(), nnz * sizeof(uint64_t),
+                                cudaMemcpyDeviceToHost, ctx->stream));
+        DT_CUDA(cudaStreamSynchronize(ctx->stream));
+        int64_t fib = 0;
+        for (int64_t e = 0; e < nnz; e++) fib += (e == 0 || hkey[e] != hkey[e - 1]);
+        if (best_fib < 0 || fib < best_fib) {
+            best_fib = fib;
+            best_F = F;
+            best_bits = bits_F;
+            best_key.swap(hkey);
+            if (hkey.size() != (size_t)nnz) hkey.resize((size_t)nnz);
+            DT_CUDA(cudaMemcpyAsync(best_ids.data(), ids_s.get(), nnz * sizeof(int32_t),
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+            DT_CUDA(cudaStreamSynchronize(ctx->stream));
+        }
+    }
+    hkey.clear();
+    hkey.shrink_to_fit();
+    mc.fmode = best_F;
+    const int E = oth[0] == best_F ? oth[1] : oth[0];
+    const uint64_t fmask = (uint64_t(1) << best_bits) - 1;
+
+    // Rows, (sub-)fibres in length order padded to groups of four, and the
+    // permuted nonzero order.
+    struct Fib {
+        int64_t beg;
+        int32_t len, idx;
+    };
+    std::vector<int32_t> rows, row_grp, grp_row, fib_idx, fib_ptr, order;
+    fib_idx.reserve((size_t)best_fib * 5 / 4 + 16);
+    fib_ptr.reserve((size_t)best_fib * 5 / 4 + 17);
+    order.reserve((size_t)nnz);
+    std::vector<Fib> rf;
+    int64_t e = 0;
+    while (e < nnz) {
+        const uint64_t r = best_key[e] >> best_bits;
+        rf.clear();
+        while (e < nnz && (best_key[e] >> best_bits) == r) {
+            const uint64_t kf = best_key[e];
+            const int64_t b = e;
+            while (e < nnz && best_key[e] == kf) e++;
+            for (int64_t s = b; s < e; s += FIB_CHUNK)
+                rf.push_back({s, (int32_t)std::min<int64_t>(FIB_CHUNK, e - s),
+                              (int32_t)(kf & fmask)});
+        }
+        std::stable_sort(rf.begin(), rf.end(),
+                         [](const Fib &a, const Fib &b) { return a.len > b.len; });
+        while (rf.size() % 4) rf.push_back({0, 0, 0});
+        const int32_t k = (int32_t)rows.size();
+        rows.push_back((int32_t)r);
+        row_grp.push_back((int32_t)(fib_idx.size() / 4));
+        for (const Fib &f : rf) {
+            fib_idx.push_back(f.idx);
+            fib_ptr.push_back((int32_t)order.size());
+            for (int32_t j = 0; j < f.len; j++) order.push_back(best_ids[f.beg + j]);
+        }
+        for (size_t q = 0; q < rf.size() / 4; q++) grp_row.push_back(k);
+    }
+    const int32_t ngroups = (int32_t)(fib_idx.size() / 4);
+    row_grp.push_back(ngroups);
+    grp_row.push_back(-1);
+    fib_ptr.push_back((int32_t)order.size());
+    best_key.clear();
+    best_key.shrink_to_fit();
+    mc.nrows = (int64_t)rows.size();
+    mc.nfib = (int64_t)fib_idx.size();
+
+    // Tasks over groups: packs of whole rows up to TASK_PACK_GRP groups; longer
+    // rows in pieces of TASK_PIECE_GRP groups writing partial rows.  Each task
+    // is cut into batches of at most FB_GRP groups and FB_NZ nonzeros (a group
+    // holds at most 4 FIB_CHUNK <= FB_NZ).  Cost estimate for the
+    // largest-first order: nonzeros + 16 per group.
+    auto gnz = [&](int32_t q) { return fib_ptr[4 * q + 4] - fib_ptr[4 * q]; };
+    std::vector<int2> bt;
     struct Task {
-        int64_t beg, end;
-        int32_t row, slot;
+        int4 t;
+        int64_t cost;
     };
     std::vector<Task> tasks;
     std::vector<int32_t> tmrow, tmfirst, tmcount;
     int64_t tslots = 0;
+    auto add_task = [&](int32_t q0, int32_t q1, int32_t slot) {
+        const int32_t b0 = (int32_t)bt.size();
+        int32_t q = q0;
+        while (q < q1) {
+            bt.push_back(make_int2(q, fib_ptr[4 * q]));
+            int32_t nz = 0, cnt = 0;
+            while (q < q1 && cnt < FB_GRP && nz + gnz(q) <= FB_NZ) {
+                nz += gnz(q);
+                cnt++;
+                q++;
+            }
+        }
+        const int64_t cost = (int64_t)(fib_ptr[4 * q1] - fib_ptr[4 * q0]) + 16 * (int64_t)(q1 - q0);
+        tasks.push_back({make_int4(b0, (int32_t)bt.size(), slot, 0), cost});
+    };
     {
-        int64_t pack_beg = -1;
-        int32_t pack_row = 0;
-        auto close_pack = [&](int64_t e) {
-            if (pack_beg >= 0) tasks.push_back({pack_beg, e, pack_row, -1});
-            pack_beg = -1;
-        };
+        int32_t pack_beg = -1;
         for (int64_t k = 0; k < mc.nrows; k++) {
-            const int64_t b = rowptr[k], c = rowptr[k + 1] - b;
-            if (c > TASK_PACK) {
-                close_pack(b);
-                const int64_t np = (c + TASK_PIECE - 1) / TASK_PIECE;
+            const int32_t b = row_grp[k], c = row_grp[k + 1] - b;
+            if (c > TASK_PACK_GRP) {
+                if (pack_beg >= 0) add_task(pack_beg, b, -1);
+                pack_beg = -1;
+                const int32_t np = (int32_t)((c + TASK_PIECE_GRP - 1) / TASK_PIECE_GRP);
                 if (np > 1) {
                     tmrow.push_back((int32_t)k);
                     tmfirst.push_back((int32_t)tslots);
-                    tmcount.push_back((int32_t)np);
+                    tmcount.push_back(np);
                 }
-                for (int64_t j = 0; j < np; j++)
-                    tasks.push_back({b + j * TASK_PIECE, std::min(b + c, b + (j + 1) * TASK_PIECE),
-                                     (int32_t)k, np > 1 ? (int32_t)(tslots + j) : -1});
+                for (int32_t j = 0; j < np; j++) {
+                    const int32_t q0 = b + j * (int32_t)TASK_PIECE_GRP;
+                    const int32_t q1 = std::min(b + c, q0 + (int32_t)TASK_PIECE_GRP);
+                    add_task(q0, q1, np > 1 ? (int32_t)(tslots + j) : -1);
+                }
                 if (np > 1) tslots += np;
                 continue;
             }
-            if (pack_beg >= 0 && b + c - pack_beg > TASK_PACK) close_pack(b);
-            if (pack_beg < 0) {
-                pack_beg = b;
-                pack_row = (int32_t)k;
+            if (pack_beg >= 0 && b + c - pack_beg > TASK_PACK_GRP) {
+                add_task(pack_beg, b, -1);
+                pack_beg = -1;
             }
+            if (pack_beg < 0) pack_beg = b;
         }
-        close_pack(nnz);
-        std::stable_sort(tasks.begin(), tasks.end(), [](const Task &a, const Task &b) {
-            return a.end - a.beg > b.end - b.beg;
-        });
+        if (pack_beg >= 0) add_task(pack_beg, ngroups, -1);
+        bt.push_back(make_int2(ngroups, fib_ptr[4 * ngroups]));
+        std::stable_sort(tasks.begin(), tasks.end(),
+                         [](const Task &a, const Task &b) { return a.cost > b.cost; });
     }
-    mc.ntasks = (int64_t)tasks.size();
+    std::vector<int4> tv(tasks.size());
+    for (size_t i = 0; i < tasks.size(); i++) tv[i] = tasks[i].t;
+    mc.ntasks = (int64_t)tv.size();
+    mc.nbatch = (int64_t)bt.size() - 1;
     mc.tslots = tslots;
     mc.tmulti = (int64_t)tmrow.size();
-    std::vector<int64_t> tbeg(tasks.size()), tend(tasks.size());
-    std::vector<int32_t> trow(tasks.size()), tslot(tasks.size());
-    for (size_t i = 0; i < tasks.size(); i++) {
-        tbeg[i] = tasks[i].beg;
-        tend[i] = tasks[i].end;
-        trow[i] = tasks[i].row;
-        tslot[i] = tasks[i].slot;
-    }
-    auto up = [&](DevMem &dst, const void *src, size_t bytes) {
-        dst.alloc(ctx, std::max<size_t>(bytes, 8));
-        if (bytes)
-            DT_CUDA(cudaMemcpyAsync(dst.get(), src, bytes, cudaMemcpyHostToDevice, ctx->stream));
-    };
-    up(mc.rows, rows.data(), rows.size() * sizeof(int32_t));
-    up(mc.rowptr, rowptr.data(), rowptr.size() * sizeof(int64_t));
-    up(mc.chunk_row, crow.data(), crow.size() * sizeof(int32_t));
-    up(mc.chunk_beg, cbeg.data(), cbeg.size() * sizeof(int64_t));
-    up(mc.chunk_slot, cslot.data(), cslot.size() * sizeof(int32_t));
-    up(mc.multi_row, mrow.data(), mrow.size() * sizeof(int32_t));
-    up(mc.multi_first, mfirst.data(), mfirst.size() * sizeof(int32_t));
-    up(mc.multi_count, mcount.data(), mcount.size() * sizeof(int32_t));
-    up(mc.task_beg, tbeg.data(), tbeg.size() * sizeof(int64_t));
-    up(mc.task_end, tend.data(), tend.size() * sizeof(int64_t));
-    up(mc.task_row, trow.data(), trow.size() * sizeof(int32_t));
-    up(mc.task_slot, tslot.data(), tslot.size() * sizeof(int32_t));
-    up(mc.tmulti_row, tmrow.data(), tmrow.size() * sizeof(int32_t));
-    up(mc.tmulti_first, tmfirst.data(), tmfirst.size() * sizeof(int32_t));
-    up(mc.tmulti_count, tmcount.data(), tmcount.size() * sizeof(int32_t));
+
+    DevMem perm;
+    upload(ctx, perm, order);
+    mc.e_idx.alloc(ctx, nnz * sizeof(int32_t));
+    mc.e_val.alloc(ctx, nnz * sizeof(double));
+    DT_LAUNCH(ctx, gather_kernel<int32_t>, blocks, 256, 0, idx32[E].as<int32_t>(),
+              perm.as<int32_t>(), nnz, mc.e_idx.as<int32_t>());
+    DT_LAUNCH(ctx, gather_kernel<double>, blocks, 256, 0, vals_dev, perm.as<int32_t>(), nnz,
+              mc.e_val.as<double>());
+    upload(ctx, mc.rows, rows);
+    upload(ctx, mc.grp_row, grp_row);
+    upload(ctx, mc.fib_idx, fib_idx);
+    upload(ctx, mc.fib_ptr, fib_ptr);
+    upload(ctx, mc.batches, bt);
+    upload(ctx, mc.tasks, tv);
+    upload(ctx, mc.tmulti_row, tmrow);
+    upload(ctx, mc.tmulti_first, tmfirst);
+    upload(ctx, mc.tmulti_count, tmcount);
     DT_CUDA(cudaStreamSynchronize(ctx->stream));
 }
 
-template <int PL, bool FAST3>
+void build_mode(dt_ctx *ctx, dt_sptensor *sp, int n, const std::vector<DevMem> &idx32,
+                const double *vals_dev) {
+    if (sp->ndim == 3)
+        build_mode_fibre(ctx, sp, n, idx32, vals_dev);
+    else
+        build_mode_rows(ctx, sp, n, idx32, vals_dev);
+}
+
+template <int PL>
 void launch_rows(dt_ctx *ctx, const ModeCopy &mc, int nother, int64_t nnz, const FactorSet &f,
                  int P, double *Yc, double *Ypart) {
     const int64_t warps = mc.nchunks;
     const unsigned blocks =
         std::max(1u, std::min<unsigned>(ceil_div(warps, 8), 32u * (unsigned)ctx->num_sms));
-    DT_LAUNCH(ctx, (ttmc_rows_kernel<PL, FAST3>), blocks, 256, 0, mc.other.as<int32_t>(),
+    DT_LAUNCH(ctx, ttmc_rows_kernel<PL>, blocks, 256, 0, mc.other.as<int32_t>(),
               mc.val.as<double>(), nnz, nother, mc.rowptr.as<int64_t>(),
               mc.chunk_row.as<int32_t>(), mc.chunk_beg.as<int64_t>(),
               mc.chunk_slot.as<int32_t>(), mc.nchunks, f, P, Yc, Ypart);
 }
 
-template <int RA, int RB, int AW, int BW>
-void launch_t3(dt_ctx *ctx, const ModeCopy &mc, int64_t nnz, const FactorSet &f, double *Yc,
-               double *Ypart) {
-    using C = T3<RA, RB, AW, BW>;
-    const size_t smem = (size_t)T3_WARPS * C::WARP_SMEM * sizeof(double);
-    auto kern = ttmc3_kernel<RA, RB, AW, BW>;
+template <int TF, int TE, bool FLO>
+void launch_fib(dt_ctx *ctx, const ModeCopy &mc, const double *UF, int RF, const double *UE,
+                int RE, double *Yc, double *Ypart) {
+    using S = FbStage<TF, TE>;
+    auto kern = ttmc3f_kernel<TF, TE, FLO>;
+    // Two CTAs per SM when their stages fit in half of the 228 KB (1 KB of
+    // each CTA's share is reserved), else one.
+    int per_sm = 2, warps = std::min(8, (228 * 1024 / 2 - 1024) / S::WARP_BYTES);
+    if (warps < 1) {
+        per_sm = 1;
+        warps = std::max(1, std::min(8, (227 * 1024) / S::WARP_BYTES));
+    }
+    const size_t smem = (size_t)warps * S::WARP_BYTES;
     smem_limit(ctx, kern, smem);
-    const int per_sm = std::max<int>(1, std::min<int>(8, (int)((220 * 1024) / smem)));
     const unsigned blocks = (unsigned)std::max<int64_t>(
-        1, std::min<int64_t>((mc.ntasks + T3_WARPS - 1) / T3_WARPS, (int64_t)per_sm * ctx->num_sms));
-    DT_LAUNCH(ctx, kern, blocks, T3_WARPS * 32, smem, mc.other.as<int32_t>(),
-              mc.other.as<int32_t>() + nnz, mc.val.as<double>(), mc.rowptr.as<int64_t>(),
-              mc.nrows, mc.task_beg.as<int64_t>(), mc.task_end.as<int64_t>(),
-              mc.task_row.as<int32_t>(), mc.task_slot.as<int32_t>(), mc.ntasks, f.U[0], f.U[1],
-              Yc, Ypart);
+        1, std::min<int64_t>((mc.ntasks + warps - 1) / warps, (int64_t)per_sm * ctx->num_sms));
+    DevMem next(ctx, sizeof(int));
+    DT_CUDA(cudaMemsetAsync(next.get(), 0, sizeof(int), ctx->stream));
+    DT_LAUNCH(ctx, kern, blocks, warps * 32, smem, mc.tasks.as<int4>(), mc.ntasks,
+              mc.batches.as<int2>(), mc.grp_row.as<int32_t>(), mc.fib_idx.as<int32_t>(),
+              mc.fib_ptr.as<int32_t>(), mc.e_idx.as<int32_t>(), mc.e_val.as<double>(), UF, RF,
+              UE, RE, Yc, Ypart, next.as<int>());
 }
 
-// The 3-way task kernel for the rank pairs it is instantiated for; false if
-// (Ra, Rb) is not one of them.
-bool ttmc3_dispatch(dt_ctx *ctx, const ModeCopy &mc, int64_t nnz, const FactorSet &f, double *Yc,
-                    double *Ypart) {
-    const int a = f.R[0], b = f.R[1];
-#define DT_T3(RA, RB, AW, BW)                                        \
-    if (a == RA && b == RB) {                                        \
-        launch_t3<RA, RB, AW, BW>(ctx, mc, nnz, f, Yc, Ypart);       \
-        return true;                                                 \
+template <int PL, bool FLO>
+void launch_fib_wide(dt_ctx *ctx, const ModeCopy &mc, const double *UF, int RF, const double *UE,
+                     int RE, double *Yc, double *Ypart) {
+    auto kern = ttmc3f_wide_kernel<PL, FLO>;
+    const unsigned blocks = (unsigned)std::max<int64_t>(
+        1, std::min<int64_t>((mc.ntasks + 7) / 8, (int64_t)8 * ctx->num_sms));
+    DT_LAUNCH(ctx, kern, blocks, 256, 0, mc.tasks.as<int4>(), mc.ntasks, mc.batches.as<int2>(),
+              mc.grp_row.as<int32_t>(), mc.fib_idx.as<int32_t>(), mc.fib_ptr.as<int32_t>(),
+              mc.e_idx.as<int32_t>(), mc.e_val.as<double>(), UF, RF, UE, RE, Yc, Ypart);
+}
+
+template <int TF, bool FLO>
+void fib_dispatch_te(dt_ctx *ctx, const ModeCopy &mc, const double *UF, int RF, const double *UE,
+                     int RE, double *Yc, double *Ypart) {
+    switch ((RE + 7) / 8) {
+        case 1: launch_fib<TF, 1, FLO>(ctx, mc, UF, RF, UE, RE, Yc, Ypart); break;
+        case 2: launch_fib<TF, 2, FLO>(ctx, mc, UF, RF, UE, RE, Yc, Ypart); break;
+        case 3: launch_fib<TF, 3, FLO>(ctx, mc, UF, RF, UE, RE, Yc, Ypart); break;
+        default: launch_fib<TF, 4, FLO>(ctx, mc, UF, RF, UE, RE, Yc, Ypart); break;
     }
-    DT_T3(16, 16, 2, 4)
-    DT_T3(8, 8, 1, 2)
-    DT_T3(32, 32, 2, 4)
-    DT_T3(16, 8, 1, 4)
-    DT_T3(8, 16, 1, 4)
-    DT_T3(10, 10, 1, 2)
-    DT_T3(12, 12, 1, 4)
-    DT_T3(4, 4, 1, 2)
-#undef DT_T3
-    return false;
+}
+
+template <bool FLO>
+void fib_dispatch(dt_ctx *ctx, const ModeCopy &mc, const double *UF, int RF, const double *UE,
+                  int RE, double *Yc, double *Ypart) {
+    if (RF > 32 || RE > 32) {
+        const int PL = (RF * RE + 31) / 32;
+        if (PL <= 8) launch_fib_wide<8, FLO>(ctx, mc, UF, RF, UE, RE, Yc, Ypart);
+        else if (PL <= 16) launch_fib_wide<16, FLO>(ctx, mc, UF, RF, UE, RE, Yc, Ypart);
+        else launch_fib_wide<32, FLO>(ctx, mc, UF, RF, UE, RE, Yc, Ypart);
+        return;
+    }
+    switch ((RF + 7) / 8) {
+        case 1: fib_dispatch_te<1, FLO>(ctx, mc, UF, RF, UE, RE, Yc, Ypart); break;
+        case 2: fib_dispatch_te<2, FLO>(ctx, mc, UF, RF, UE, RE, Yc, Ypart); break;
+        case 3: fib_dispatch_te<3, FLO>(ctx, mc, UF, RF, UE, RE, Yc, Ypart); break;
+        default: fib_dispatch_te<4, FLO>(ctx, mc, UF, RF, UE, RE, Yc, Ypart); break;
+    }
 }
 
 }  // namespace
@@ -776,6 +1105,38 @@ void sp_ttmc_compact(dt_ctx *ctx, const dt_sptensor *sp, const double *const *Ut
     DT_CHECK_ARG(P64 <= 1024, "sparse TTMc: prod of the other ranks (%lld) exceeds 1024",
                  (long long)P64);
     const int P = (int)P64;
+    if (nd == 3) {
+        const int F = mc.fmode;
+        int E = 0;
+        for (int m = 0; m < 3; m++)
+            if (m != mode && m != F) E = m;
+        DevMem tpart(ctx, std::max<int64_t>(mc.tslots, 1) * P * sizeof(double));
+        if (timer) timer->begin();
+        if (F < E)
+            fib_dispatch<true>(ctx, mc, Ut_dev[F], (int)R[F], Ut_dev[E], (int)R[E], Yc,
+                               tpart.as<double>());
+        else
+            fib_dispatch<false>(ctx, mc, Ut_dev[F], (int)R[F], Ut_dev[E], (int)R[E], Yc,
+                                tpart.as<double>());
+        if (mc.tmulti > 0) {
+            const unsigned blocks = (unsigned)std::min<int64_t>(mc.tmulti, 65535);
+            DT_LAUNCH(ctx, combine_partials_kernel, blocks, 256 * COMB_SPLIT, 0,
+                      tpart.as<double>(), mc.tmulti_row.as<int32_t>(),
+                      mc.tmulti_first.as<int32_t>(), mc.tmulti_count.as<int32_t>(), mc.tmulti, P,
+                      Yc);
+        }
+        if (timer) {
+            // Bytes this layout must move: per nonzero its i_E (int32) and
+            // value, per fibre its i_F and pointer (int32), each other factor
+            // once, and the compact Y_(n) rows written.
+            const double bytes = (double)sp->nnz * 12.0 + (double)mc.nfib * 8.0 +
+                                 (double)mc.nrows * P * 8.0 +
+                                 (double)sp->shape[F] * R[F] * 8.0 +
+                                 (double)sp->shape[E] * R[E] * 8.0;
+            timer->end(bytes);
+        }
+        return;
+    }
     FactorSet f{};
     int d = 0;
     for (int m = 0; m < nd; m++) {
@@ -784,47 +1145,18 @@ void sp_ttmc_compact(dt_ctx *ctx, const dt_sptensor *sp, const double *const *Ut
         f.R[d] = (int)R[m];
         d++;
     }
-    if (nd == 3 && mc.ntasks > 0) {
-        DevMem tpart(ctx, std::max<int64_t>(mc.tslots, 1) * P * sizeof(double));
-        if (timer) timer->begin();
-        if (ttmc3_dispatch(ctx, mc, sp->nnz, f, Yc, tpart.as<double>())) {
-            if (mc.tmulti > 0) {
-                const unsigned blocks = (unsigned)std::min<int64_t>(mc.tmulti, 65535);
-                DT_LAUNCH(ctx, combine_partials_kernel, blocks, 256, 0, tpart.as<double>(),
-                          mc.tmulti_row.as<int32_t>(), mc.tmulti_first.as<int32_t>(),
-                          mc.tmulti_count.as<int32_t>(), mc.tmulti, P, Yc);
-            }
-            if (timer) {
-                double bytes = (double)sp->nnz * (4.0 * (nd - 1) + 8.0) + (double)mc.nrows * P * 8.0;
-                for (int m = 0; m < nd; m++)
-                    if (m != mode) bytes += (double)sp->shape[m] * R[m] * 8.0;
-                timer->end(bytes);
-            }
-            return;
-        }
-    }
     DevMem part(ctx, std::max<int64_t>(mc.nslots, 1) * P * sizeof(double));
     if (timer) timer->begin();
-    const bool fast3 = nd == 3 && f.R[0] <= 32 && (32 % f.R[0]) == 0 && f.R[1] <= 32;
     const int PL = (P + 31) / 32;
-    if (fast3) {
-        if (PL <= 1) launch_rows<1, true>(ctx, mc, nd - 1, sp->nnz, f, P, Yc, part.as<double>());
-        else if (PL <= 2) launch_rows<2, true>(ctx, mc, nd - 1, sp->nnz, f, P, Yc, part.as<double>());
-        else if (PL <= 4) launch_rows<4, true>(ctx, mc, nd - 1, sp->nnz, f, P, Yc, part.as<double>());
-        else if (PL <= 8) launch_rows<8, true>(ctx, mc, nd - 1, sp->nnz, f, P, Yc, part.as<double>());
-        else if (PL <= 16) launch_rows<16, true>(ctx, mc, nd - 1, sp->nnz, f, P, Yc, part.as<double>());
-        else launch_rows<32, true>(ctx, mc, nd - 1, sp->nnz, f, P, Yc, part.as<double>());
-    } else {
-        if (PL <= 1) launch_rows<1, false>(ctx, mc, nd - 1, sp->nnz, f, P, Yc, part.as<double>());
-        else if (PL <= 2) launch_rows<2, false>(ctx, mc, nd - 1, sp->nnz, f, P, Yc, part.as<double>());
-        else if (PL <= 4) launch_rows<4, false>(ctx, mc, nd - 1, sp->nnz, f, P, Yc, part.as<double>());
-        else if (PL <= 8) launch_rows<8, false>(ctx, mc, nd - 1, sp->nnz, f, P, Yc, part.as<double>());
-        else if (PL <= 16) launch_rows<16, false>(ctx, mc, nd - 1, sp->nnz, f, P, Yc, part.as<double>());
-        else launch_rows<32, false>(ctx, mc, nd - 1, sp->nnz, f, P, Yc, part.as<double>());
-    }
+    if (PL <= 1) launch_rows<1>(ctx, mc, nd - 1, sp->nnz, f, P, Yc, part.as<double>());
+    else if (PL <= 2) launch_rows<2>(ctx, mc, nd - 1, sp->nnz, f, P, Yc, part.as<double>());
+    else if (PL <= 4) launch_rows<4>(ctx, mc, nd - 1, sp->nnz, f, P, Yc, part.as<double>());
+    else if (PL <= 8) launch_rows<8>(ctx, mc, nd - 1, sp->nnz, f, P, Yc, part.as<double>());
+    else if (PL <= 16) launch_rows<16>(ctx, mc, nd - 1, sp->nnz, f, P, Yc, part.as<double>());
+    else launch_rows<32>(ctx, mc, nd - 1, sp->nnz, f, P, Yc, part.as<double>());
     if (mc.nmulti > 0) {
         const unsigned blocks = (unsigned)std::min<int64_t>(mc.nmulti, 65535);
-        DT_LAUNCH(ctx, combine_partials_kernel, blocks, 256, 0, part.as<double>(),
+        DT_LAUNCH(ctx, combine_partials_kernel, blocks, 256 * COMB_SPLIT, 0, part.as<double>(),
                   mc.multi_row.as<int32_t>(), mc.multi_first.as<int32_t>(),
                   mc.multi_count.as<int32_t>(), mc.nmulti, P, Yc);
     }
