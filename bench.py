@@ -215,21 +215,24 @@ def run_ours(args):
     _, _, rep = mixed(profile=True)
 
     _log(f"mixed {ms:.3f} ms/decomposition; FP64 path")
-    # FP64 GPU path, same tensor and stopping rule: X stored in FP64 (the
-    # drop-in's Tensor<double>) and, for reference, FP64 arithmetic reading
-    # the FP32-stored X.
-    fp64()
-    t64 = []
-    for _ in range(max(1, min(args.steps, 3))):
-        _, _, r64 = fp64()
-        t64.append(r64["device_ms"])
-    fp64_ms = float(np.median(t64))
-    fp64(x=Xd)
-    t32 = []
-    for _ in range(max(1, min(args.steps, 3))):
-        _, _, r32 = fp64(x=Xd)
-        t32.append(r32["device_ms"])
-    fp64_x32_ms = float(np.median(t32))
+    # FP64 GPU path, same tensor and stopping rule, timed the same way (CUDA
+    # events around whole calls): X stored in FP64 (the drop-in's
+    # Tensor<double>) and, for reference, FP64 arithmetic reading the
+    # FP32-stored X.
+    def bracket(fn, n):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(n):
+            _, _, r = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n, r
+
+    n64 = max(1, min(args.steps, 3))
+    fp64_ms, r64 = bracket(fp64, n64)
+    fp64_x32_ms, _ = bracket(lambda: fp64(x=Xd), n64)
     del X64d
 
     _log("end to end from pinned host memory")

@@ -9,6 +9,8 @@
 #include <cstdio>
 #include <stdexcept>
 #include <string>
+#include <functional>
+#include <memory>
 #include <unordered_set>
 #include <vector>
 
@@ -27,6 +29,10 @@ struct dt_ctx {
     int num_sms = 0;
     int64_t launches = 0;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    // The dense HOOI drivers' last plans (device buffers plus a captured graph
+    // of one sweep), reused by the next call with the same shapes, ranks and
+    // options; released before the stream at dt_ctx_destroy.
+    std::shared_ptr<void> hooi_plan_fp64, hooi_plan_mixed;
 };
 
 namespace dt {
@@ -138,6 +144,31 @@ template <class K>
 inline void smem_limit(dt_ctx *ctx, K *kernel, size_t bytes) {
     raise_smem_limit(ctx, reinterpret_cast<const void *>(kernel), bytes);
 }
+
+// One launch sequence (a HOOI sweep) captured as a CUDA graph and replayed on
+// ctx->stream.  Capture fails over to direct execution: run() then calls fn()
+// itself (the capture executed nothing).  Graphs are not used on the legacy
+// or per-thread default streams, or when DT_DISABLE_GRAPHS=1.
+class SweepGraph {
+   public:
+    SweepGraph() = default;
+    SweepGraph(const SweepGraph &) = delete;
+    SweepGraph &operator=(const SweepGraph &) = delete;
+    ~SweepGraph() { reset(); }
+    void reset();
+    // Executes fn's launches: from the graph when it exists, else by capturing
+    // fn into it first; falls back to calling fn directly.
+    void run(dt_ctx *ctx, const std::function<void()> &fn);
+    bool captured() const { return exec_ != nullptr; }
+
+   private:
+    cudaGraphExec_t exec_ = nullptr;
+    int64_t launches_ = 0;
+    bool failed_ = false;
+};
+
+// Drops a cached HOOI plan once the work queued on ctx->stream is done.
+void release_plan(dt_ctx *ctx, std::shared_ptr<void> &plan);
 
 // Frees the device memory of every sparse tensor still attached to ctx and
 // detaches it (called by dt_ctx_destroy).

@@ -40,6 +40,72 @@ bool pdl_enabled() {
     return on;
 }
 
+namespace {
+bool graphs_enabled() {
+    static const bool on = [] {
+        const char *e = std::getenv("DT_DISABLE_GRAPHS");
+        return !(e && e[0] == '1');
+    }();
+    return on;
+}
+}  // namespace
+
+void release_plan(dt_ctx *ctx, std::shared_ptr<void> &plan) {
+    if (!plan) return;
+    DT_CUDA(cudaStreamSynchronize(ctx->stream));
+    plan.reset();
+}
+
+void SweepGraph::reset() {
+    if (exec_) cudaGraphExecDestroy(exec_);
+    exec_ = nullptr;
+    launches_ = 0;
+}
+
+void SweepGraph::run(dt_ctx *ctx, const std::function<void()> &fn) {
+    const bool plain_stream = ctx->stream != nullptr && ctx->stream != cudaStreamLegacy &&
+                              ctx->stream != cudaStreamPerThread;
+    if (!exec_) {
+        if (failed_ || !plain_stream || !graphs_enabled()) {
+            fn();
+            return;
+        }
+        const int64_t l0 = ctx->launches;
+        auto give_up = [&](cudaGraph_t g) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            ctx->launches = l0;
+            failed_ = true;
+        };
+        DT_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
+        cudaGraph_t g = nullptr;
+        try {
+            fn();
+        } catch (...) {
+            cudaStreamEndCapture(ctx->stream, &g);
+            give_up(g);
+            fn();
+            return;
+        }
+        if (cudaStreamEndCapture(ctx->stream, &g) != cudaSuccess || !g) {
+            give_up(g);
+            fn();
+            return;
+        }
+        if (cudaGraphInstantiateWithFlags(&exec_, g, 0) != cudaSuccess) {
+            exec_ = nullptr;
+            give_up(g);
+            fn();
+            return;
+        }
+        cudaGraphDestroy(g);
+        launches_ = ctx->launches - l0;
+        ctx->launches = l0;
+    }
+    DT_CUDA(cudaGraphLaunch(exec_, ctx->stream));
+    ctx->launches += launches_;
+}
+
 void raise_smem_limit(dt_ctx *ctx, const void *kernel, size_t bytes) {
     static std::mutex mu;
     static std::map<std::pair<const void *, int>, size_t> limits;
@@ -132,6 +198,9 @@ int dt_ctx_destroy(dt_ctx *ctx) {
         if (!ctx) return;
         cudaSetDevice(ctx->device);
         detach_sptensors(ctx);
+        if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+        ctx->hooi_plan_fp64.reset();
+        ctx->hooi_plan_mixed.reset();
         if (ctx->stream) cudaStreamSynchronize(ctx->stream);
         if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
         if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);

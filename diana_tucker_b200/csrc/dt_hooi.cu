@@ -73,20 +73,24 @@ void DenseHooi::setup(dt_ctx *c, const void *X, int dt, int n, const int64_t *sh
     }
     xsize = prod(I, N);
     Xdev = X;
-    U.resize(N);
-    for (int m = 0; m < N; m++) U[m].alloc(ctx, I[m] * R[m] * sizeof(double));
-    int64_t maxI = 0, maxR = 0;
-    for (int m = 0; m < N; m++) {
-        maxI = std::max(maxI, I[m]);
-        maxR = std::max(maxR, R[m]);
+    if (!allocated) {
+        U.resize(N);
+        for (int m = 0; m < N; m++) U[m].alloc(ctx, I[m] * R[m] * sizeof(double));
+        int64_t maxI = 0, maxR = 0;
+        for (int m = 0; m < N; m++) {
+            maxI = std::max(maxI, I[m]);
+            maxR = std::max(maxR, R[m]);
+        }
+        S.alloc(ctx, maxI * maxI * sizeof(double));
+        work.alloc(ctx, (3 * maxI * maxR + maxR + 64) * sizeof(double));
+        flag.alloc(ctx, sizeof(int));
+        scal.alloc(ctx, 4 * sizeof(double));
+        G.alloc(ctx, prod(R, N) * sizeof(double));
+        allocated = true;
     }
-    S.alloc(ctx, maxI * maxI * sizeof(double));
-    work.alloc(ctx, (3 * maxI * maxR + maxR + 64) * sizeof(double));
-    flag.alloc(ctx, sizeof(int));
-    scal.alloc(ctx, 4 * sizeof(double));
     DT_CUDA(cudaMemsetAsync(flag.get(), 0, sizeof(int), ctx->stream));
     if (dtype == DT_F32 && N == 1) {
-        X64.alloc(ctx, xsize * sizeof(double));
+        if (!X64.get()) X64.alloc(ctx, xsize * sizeof(double));
         f32_to_f64(ctx, static_cast<const float *>(X), xsize, X64.as<double>());
         Xdev = X64.get();
         dtype = DT_F64;
@@ -141,7 +145,6 @@ void DenseHooi::leaf(int n, const double *Y, const int64_t *shape) {
                   work.as<double>(), flag.as<int>());
     if (n == N - 1) {
         // Core of this sweep: G = Y x_{N-1} U_{N-1}^T (hooi_als.tpp:105-109).
-        G.alloc(ctx, L * R[n] * sizeof(double));
         ttm_f64<double>(ctx, Y, L, I[n], 1, U[n].as<double>(), I[n], 1, R[n], G.as<double>());
         sumsq(ctx, G.get(), DT_F64, L * R[n], scal.as<double>() + 1);
     }
@@ -242,7 +245,8 @@ double DenseHooi::read_scalar(int k) {
     return h;
 }
 
-void DenseHooi::run(double *G_user, double *const *U_user, dt_hooi_report *rep) {
+void DenseHooi::run(double *G_user, double *const *U_user, dt_hooi_report *rep,
+                    SweepGraph *graph) {
     const int64_t launches0 = ctx->launches;
     LaunchTimer timer(ctx, opts.profile != 0);
     xtimer = &timer;
@@ -253,7 +257,10 @@ void DenseHooi::run(double *G_user, double *const *U_user, dt_hooi_report *rep) 
     double prev = -1.0, res = 0.0;
     int sweeps = 0;
     for (int it = 0; it < opts.max_sweeps; it++) {
-        sweep();
+        if (graph && !opts.profile)
+            graph->run(ctx, [&] { sweep(); });
+        else
+            sweep();
         const double g2 = read_scalar(1);
         res = std::sqrt(std::max(0.0, 1.0 - g2 / x2));
         if (rep && it < DT_MAX_HIST) rep->res_hist[it] = res;
@@ -270,7 +277,9 @@ void DenseHooi::run(double *G_user, double *const *U_user, dt_hooi_report *rep) 
         std::memcpy(shape, I, N * sizeof(int64_t));
         std::vector<int> all(N);
         std::iota(all.begin(), all.end(), 0);
-        G = contract_all(Xdev, dtype, shape, all);
+        DevMem g0 = contract_all(Xdev, dtype, shape, all);
+        DT_CUDA(cudaMemcpyAsync(G.get(), g0.get(), prod(R, N) * sizeof(double),
+                                cudaMemcpyDeviceToDevice, ctx->stream));
         sumsq(ctx, G.get(), DT_F64, prod(R, N), scal.as<double>() + 1);
     }
     DT_CUDA(cudaEventRecord(ctx->ev_stop, ctx->stream));
@@ -311,6 +320,31 @@ void DenseHooi::run(double *G_user, double *const *U_user, dt_hooi_report *rep) 
     }
     xtimer = nullptr;
 }
+
+// The FP64 driver's buffers and sweep graph, kept on the context for the next
+// call with the same X, shapes, ranks and inner iterations.
+struct Fp64Plan {
+    const void *X;
+    int dtype, N, inner;
+    int64_t I[16], R[16];
+    DenseHooi h;
+    SweepGraph graph;
+    Fp64Plan(const void *x, int dt, int n, const int64_t *shape, const int64_t *ranks,
+             const dt_hooi_opts &o)
+        : X(x), dtype(dt), N(n), inner(o.inner_iters) {
+        for (int m = 0; m < n; m++) {
+            I[m] = shape[m];
+            R[m] = ranks[m];
+        }
+    }
+    bool matches(const void *x, int dt, int n, const int64_t *shape, const int64_t *ranks,
+                 const dt_hooi_opts &o) const {
+        if (x != X || dt != dtype || n != N || o.inner_iters != inner) return false;
+        for (int m = 0; m < n; m++)
+            if (shape[m] != I[m] || ranks[m] != R[m]) return false;
+        return true;
+    }
+};
 
 }  // namespace dt
 
@@ -355,9 +389,17 @@ int dt_hooi_dense(dt_ctx *ctx, const void *X, int dtype, int ndim, const int64_t
         const size_t esz = dtype == DT_F64 ? 8 : 4;
         DevView x(ctx, X, prod(shape, ndim) * esz, true, false);
         if (o.precision == DT_PREC_FP64) {
-            DenseHooi h;
-            h.setup(ctx, x.ptr(), dtype, ndim, shape, ranks, o);
-            h.run(G, U, report);
+            // A staged host X lives only for this call: its plan is not kept
+            // and its sweeps are launched directly.
+            const bool keep = x.ptr() == X;
+            auto plan = std::static_pointer_cast<Fp64Plan>(ctx->hooi_plan_fp64);
+            if (!keep || !plan || !plan->matches(x.ptr(), dtype, ndim, shape, ranks, o)) {
+                if (keep) release_plan(ctx, ctx->hooi_plan_fp64);
+                plan = std::make_shared<Fp64Plan>(x.ptr(), dtype, ndim, shape, ranks, o);
+                if (keep) ctx->hooi_plan_fp64 = plan;
+            }
+            plan->h.setup(ctx, x.ptr(), dtype, ndim, shape, ranks, o);
+            plan->h.run(G, U, report, keep ? &plan->graph : nullptr);
         } else {
             hooi_dense_lowprec(ctx, x.ptr(), dtype, ndim, shape, ranks, o, G, U, report);
         }

@@ -21,13 +21,20 @@ struct DenseHooi {
     DevMem X64;               // FP64 copy when needed
     std::vector<DevMem> U;    // I_n x R_n col-major
     DevMem S, work, flag, scal, G;
+    bool allocated = false;
     int hosvd_iters = 30;
     LaunchTimer *xtimer = nullptr;  // times the TTM launches that read X
 
+    // Allocates the buffers on the first call; a later call on the same
+    // object (same shapes and ranks) keeps them, so a captured sweep graph
+    // stays valid.
     void setup(dt_ctx *c, const void *X, int dtype, int n, const int64_t *shape,
                const int64_t *ranks, const dt_hooi_opts &o);
     void init_factors(double *const *U_user);
-    void run(double *G_user, double *const *U_user, dt_hooi_report *rep);
+    // graph: replays the sweep from a captured CUDA graph (null: launch
+    // directly; never used with opts.profile).
+    void run(double *G_user, double *const *U_user, dt_hooi_report *rep,
+             SweepGraph *graph = nullptr);
 
    private:
     DevMem contract(const void *t, int tdtype, int64_t *shape, int m);

@@ -45,10 +45,21 @@ struct MixedHooi {
     bool split = false;
     DenseHooi helper;  // initial factors (same generators as the FP64 driver)
     LaunchTimer *xtimer = nullptr;
+    SweepGraph *g_bf16 = nullptr, *g_split = nullptr;  // captured sweeps (or null)
 
     static std::vector<int> order_high_first(std::vector<int> modes) {
         std::sort(modes.begin(), modes.end(), [](int a, int b) { return a > b; });
         return modes;
+    }
+
+    static bool plan_ok_for(int n, const int64_t *shape, const int64_t *ranks) {
+        MixedHooi t;
+        t.N = n;
+        for (int m = 0; m < n; m++) {
+            t.I[m] = shape[m];
+            t.R[m] = ranks[m];
+        }
+        return t.plan_ok();
     }
 
     // Checks every contraction and Gram of the dimension tree against the
@@ -222,8 +233,9 @@ struct MixedHooi {
                       X32own.as<float>());
             X32 = X32own.as<float>();
         }
-        Xh.alloc(ctx, xsize * sizeof(__nv_bfloat16));
-        if (want_split) Xl.alloc(ctx, xsize * sizeof(__nv_bfloat16));
+        // Xh / Xl persist with the plan (the captured sweeps read them).
+        if (!Xh.get()) Xh.alloc(ctx, xsize * sizeof(__nv_bfloat16));
+        if (want_split && !Xl.get()) Xl.alloc(ctx, xsize * sizeof(__nv_bfloat16));
         if (dtype == DT_F64)
             sumsq(ctx, X, DT_F64, xsize, scal.as<double>());
         DevMem x2f(ctx, sizeof(double));
@@ -255,7 +267,11 @@ struct MixedHooi {
                 split = true;
                 prev = -1.0;
             }
-            sweep();
+            SweepGraph *gr = split ? g_split : g_bf16;
+            if (gr && !opts.profile)
+                gr->run(ctx, [&] { sweep(); });
+            else
+                sweep();
             const double g2 = read_scalar(1);
             res = std::sqrt(std::max(0.0, 1.0 - g2 / x2));
             if (rep && it < DT_MAX_HIST) rep->res_hist[it] = res;
@@ -284,34 +300,39 @@ struct MixedHooi {
                 }
             }
         }
-        // Final core, FP64 projection from the original X.
-        int64_t shape[16];
-        std::memcpy(shape, I, N * sizeof(int64_t));
-        std::vector<int> ord(N);
-        std::iota(ord.begin(), ord.end(), 0);
-        std::sort(ord.begin(), ord.end(), [](int a, int b) { return a > b; });
+        // Final core, FP64 projection from the original X (the returned G is
+        // X x_1 U_1^T ... x_N U_N^T to FP64 rounding).
         DevMem cur;
-        const void *src = X32;
-        bool src_f32 = true;
-        for (int m : ord) {
-            int64_t L = 1, B = 1;
-            for (int k = 0; k < m; k++) L *= shape[k];
-            for (int k = m + 1; k < N; k++) B *= shape[k];
-            DevMem nxt(ctx, L * R[m] * B * sizeof(double));
-            if (src_f32)
-                ttm_f64<float>(ctx, static_cast<const float *>(src), L, shape[m], B,
-                               U[m].as<double>(), I[m], 1, R[m], nxt.as<double>());
-            else
-                ttm_f64<double>(ctx, static_cast<const double *>(src), L, shape[m], B,
-                                U[m].as<double>(), I[m], 1, R[m], nxt.as<double>());
-            shape[m] = R[m];
-            cur = std::move(nxt);
-            src = cur.get();
-            src_f32 = false;
+        {
+            int64_t shape[16];
+            std::memcpy(shape, I, N * sizeof(int64_t));
+            std::vector<int> ord(N);
+            std::iota(ord.begin(), ord.end(), 0);
+            std::sort(ord.begin(), ord.end(), [](int a, int b) { return a > b; });
+            const void *src = X32;
+            bool src_f32 = true;
+            for (int m : ord) {
+                int64_t L = 1, B = 1;
+                for (int k = 0; k < m; k++) L *= shape[k];
+                for (int k = m + 1; k < N; k++) B *= shape[k];
+                DevMem nxt(ctx, L * R[m] * B * sizeof(double));
+                if (src_f32)
+                    ttm_f64<float>(ctx, static_cast<const float *>(src), L, shape[m], B,
+                                   U[m].as<double>(), I[m], 1, R[m], nxt.as<double>());
+                else
+                    ttm_f64<double>(ctx, static_cast<const double *>(src), L, shape[m], B,
+                                    U[m].as<double>(), I[m], 1, R[m], nxt.as<double>());
+                shape[m] = R[m];
+                cur = std::move(nxt);
+                src = cur.get();
+                src_f32 = false;
+            }
+            sumsq(ctx, cur.get(), DT_F64, prod(R, N), scal.as<double>() + 2);
         }
-        sumsq(ctx, cur.get(), DT_F64, prod(R, N), scal.as<double>() + 2);
+        const double *gsrc = cur.as<double>();
+        const int gslot = 2;
         DT_CUDA(cudaEventRecord(ctx->ev_stop, ctx->stream));
-        const double g2 = read_scalar(2);
+        const double g2 = read_scalar(gslot);
         int herr = 0;
         DT_CUDA(cudaMemcpyAsync(&herr, err.get(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         DT_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -321,7 +342,7 @@ struct MixedHooi {
         if (!std::isfinite(g2)) fail(DT_ERR_NUMERIC, "HOOI produced a non-finite core");
         if (G_user) {
             DevView g(ctx, G_user, prod(R, N) * sizeof(double), false, true);
-            DT_CUDA(cudaMemcpyAsync(g.ptr(), cur.get(), prod(R, N) * sizeof(double),
+            DT_CUDA(cudaMemcpyAsync(g.ptr(), gsrc, prod(R, N) * sizeof(double),
                                     cudaMemcpyDeviceToDevice, ctx->stream));
             g.finish();
         }
@@ -351,6 +372,27 @@ struct MixedHooi {
     }
 };
 
+// The mixed driver's buffers and captured sweeps (one graph per precision).
+struct MixedPlan {
+    int N, inner;
+    int64_t I[16], R[16];
+    MixedHooi h;
+    SweepGraph g_bf16, g_split;
+    MixedPlan(int n, const int64_t *shape, const int64_t *ranks, const dt_hooi_opts &o)
+        : N(n), inner(o.inner_iters) {
+        for (int m = 0; m < n; m++) {
+            I[m] = shape[m];
+            R[m] = ranks[m];
+        }
+    }
+    bool matches(int n, const int64_t *shape, const int64_t *ranks, const dt_hooi_opts &o) const {
+        if (n != N || o.inner_iters != inner) return false;
+        for (int m = 0; m < n; m++)
+            if (shape[m] != I[m] || ranks[m] != R[m]) return false;
+        return true;
+    }
+};
+
 }  // namespace
 
 void hooi_dense_lowprec(dt_ctx *ctx, const void *X, int dtype, int ndim, const int64_t *shape,
@@ -360,16 +402,7 @@ void hooi_dense_lowprec(dt_ctx *ctx, const void *X, int dtype, int ndim, const i
                  "unknown precision %d", opts.precision);
     DT_CHECK_ARG(opts.init != DT_INIT_HOSVD,
                  "the tensor-core HOOI starts from random or given factors, not HOSVD");
-    MixedHooi h;
-    h.ctx = ctx;
-    h.N = ndim;
-    h.opts = opts;
-    for (int m = 0; m < ndim; m++) {
-        h.I[m] = shape[m];
-        h.R[m] = ranks[m];
-    }
-    h.xsize = prod(shape, ndim);
-    if (!h.plan_ok()) {
+    if (!MixedHooi::plan_ok_for(ndim, shape, ranks)) {
         // A shape outside the TMA / UMMA layout rules: run the FP64 engine.
         dt_hooi_opts o = opts;
         o.precision = DT_PREC_FP64;
@@ -379,20 +412,41 @@ void hooi_dense_lowprec(dt_ctx *ctx, const void *X, int dtype, int ndim, const i
         if (report) report->precision_used = DT_PREC_FP64;
         return;
     }
-    h.helper.setup(ctx, X, dtype, ndim, shape, ranks, opts);
-    h.U.resize(ndim);
-    int64_t maxI = 0, maxR = 0;
-    for (int m = 0; m < ndim; m++) {
-        h.U[m].alloc(ctx, shape[m] * ranks[m] * sizeof(double));
-        maxI = std::max(maxI, shape[m]);
-        maxR = std::max(maxR, ranks[m]);
+    // The plan (buffers + captured sweeps) is kept on the context for the next
+    // call with the same shapes, ranks and inner iterations.
+    auto plan = std::static_pointer_cast<MixedPlan>(ctx->hooi_plan_mixed);
+    if (!plan || !plan->matches(ndim, shape, ranks, opts)) {
+        release_plan(ctx, ctx->hooi_plan_mixed);
+        plan = std::make_shared<MixedPlan>(ndim, shape, ranks, opts);
+        MixedHooi &h = plan->h;
+        h.ctx = ctx;
+        h.N = ndim;
+        for (int m = 0; m < ndim; m++) {
+            h.I[m] = shape[m];
+            h.R[m] = ranks[m];
+        }
+        h.xsize = prod(shape, ndim);
+        h.U.resize(ndim);
+        int64_t maxI = 0, maxR = 0;
+        for (int m = 0; m < ndim; m++) {
+            h.U[m].alloc(ctx, shape[m] * ranks[m] * sizeof(double));
+            maxI = std::max(maxI, shape[m]);
+            maxR = std::max(maxR, ranks[m]);
+        }
+        h.S.alloc(ctx, maxI * maxI * sizeof(double));
+        h.work.alloc(ctx, (3 * maxI * maxR + maxR + 64) * sizeof(double));
+        h.flag.alloc(ctx, sizeof(int));
+        h.err.alloc(ctx, sizeof(int));
+        h.scal.alloc(ctx, 4 * sizeof(double));
+        h.Gs.alloc(ctx, prod(ranks, ndim) * sizeof(double));
+        h.g_bf16 = &plan->g_bf16;
+        h.g_split = &plan->g_split;
+        ctx->hooi_plan_mixed = plan;
     }
-    h.S.alloc(ctx, maxI * maxI * sizeof(double));
-    h.work.alloc(ctx, (3 * maxI * maxR + maxR + 64) * sizeof(double));
-    h.flag.alloc(ctx, sizeof(int));
-    h.err.alloc(ctx, sizeof(int));
-    h.scal.alloc(ctx, 4 * sizeof(double));
-    h.Gs.alloc(ctx, prod(ranks, ndim) * sizeof(double));
+    MixedHooi &h = plan->h;
+    h.opts = opts;
+    h.X32 = nullptr;
+    h.helper.setup(ctx, X, dtype, ndim, shape, ranks, opts);
     DT_CUDA(cudaMemsetAsync(h.flag.get(), 0, sizeof(int), ctx->stream));
     DT_CUDA(cudaMemsetAsync(h.err.get(), 0, sizeof(int), ctx->stream));
     h.run(X, dtype, G, U, report);

@@ -61,7 +61,8 @@ struct ModeCopy {
     DevMem e_val;         // double [nnz]
     DevMem fib_idx;       // int32 [nfib]: i_F of each fibre slot (0 when empty)
     DevMem fib_ptr;       // int32 [nfib+1]: its nonzeros
-    DevMem grp_row;       // int32 [nfib/4 + 1]: compact row of each group, then -1
+    DevMem grp_row;       // int32 [nfib/4]: compact row of each group
+    DevMem grp_aux;       // int32 [nfib/4]: longest fibre | FB_ROW_END (last group of its row)
     // Batches: int2 {first group, first nonzero} (+ an end entry); a batch is
     // at most FB_GRP groups and FB_NZ nonzeros.  Tasks: int4 {first batch, end
     // batch, partial slot or -1, 0}: packs of whole consecutive rows, or pieces
@@ -222,6 +223,7 @@ __device__ __forceinline__ void sp_dmma(double &d0, double &d1, double a, double
 constexpr int FB_NZ = 32;
 constexpr int FB_GRP = 4;
 constexpr int FB_SLOTS = 4 * FB_GRP;
+constexpr int FB_ROW_END = 1 << 8;  // grp_aux: the group is the last of its row
 
 // Shared row pitch (doubles) for a staged factor row of R entries: even (16-byte
 // pieces) and 4 mod 8, so four rows read by one fragment load start in
@@ -236,7 +238,7 @@ template <int TF, int TE>
 struct FbStage {
     static constexpr int PE = fb_pitch(8 * TE), PF = fb_pitch(8 * TF);
     static constexpr int DOUBLES = FB_NZ * PE + FB_SLOTS * PF + FB_NZ;
-    static constexpr int INTS = FB_SLOTS + 1 + FB_GRP + 1;
+    static constexpr int INTS = FB_SLOTS + 1 + 2 * FB_GRP;
     static constexpr int BYTES = DOUBLES * 8 + ((INTS * 4 + 15) & ~15);
     static constexpr int WARP_BYTES = 2 * BYTES;
 };
@@ -257,17 +259,18 @@ __device__ __forceinline__ void sp_cp_wait() {
 
 struct FbMeta {
     int g0, ng, nz0, nzn;
-    int fidx, fofs, grow;
+    int fidx, fofs, grow, gaux;
     int idx;
     double v;
 };
 
 // Registers of batch b: lane l holds fibre slot l (index, offset into the
-// batch's nonzeros), nonzero l (index, value) and the row of group l (l <= ng;
-// the entry after the batch tells whether its last group ends a row).
+// batch's nonzeros), nonzero l (index, value) and group l's row and aux word
+// (longest fibre | FB_ROW_END when the group is the last of its row).
 __device__ __forceinline__ void fb_load_meta(FbMeta &m, int b, int lane,
                                              const int2 *__restrict__ bt,
                                              const int32_t *__restrict__ grp_row,
+                                             const int32_t *__restrict__ grp_aux,
                                              const int32_t *__restrict__ fib_idx,
                                              const int32_t *__restrict__ fib_ptr,
                                              const int32_t *__restrict__ e_idx,
@@ -280,7 +283,8 @@ __device__ __forceinline__ void fb_load_meta(FbMeta &m, int b, int lane,
     const bool sv = lane < 4 * m.ng;
     m.fidx = sv ? fib_idx[4 * m.g0 + lane] : 0;
     m.fofs = sv ? fib_ptr[4 * m.g0 + lane] - m.nz0 : 0;
-    m.grow = lane <= m.ng ? grp_row[m.g0 + lane] : -1;
+    m.grow = lane < m.ng ? grp_row[m.g0 + lane] : 0;
+    m.gaux = lane < m.ng ? grp_aux[m.g0 + lane] : 0;
     const bool a = lane < m.nzn;
     m.idx = a ? e_idx[m.nz0 + lane] : 0;
     m.v = a ? e_val[m.nz0 + lane] : 0.0;
@@ -323,11 +327,11 @@ __device__ __forceinline__ void fb_stage_rows(double *dst, int pitch, const doub
 template <int TF, int TE, bool FLO>
 __global__ void __launch_bounds__(256, 2) ttmc3f_kernel(
     const int4 *__restrict__ tasks, int64_t ntasks, const int2 *__restrict__ bt,
-    const int32_t *__restrict__ grp_row, const int32_t *__restrict__ fib_idx,
-    const int32_t *__restrict__ fib_ptr, const int32_t *__restrict__ e_idx,
-    const double *__restrict__ e_val, const double *__restrict__ UF, int RF,
-    const double *__restrict__ UE, int RE, double *__restrict__ Yc, double *__restrict__ Ypart,
-    int *__restrict__ next_task) {
+    const int32_t *__restrict__ grp_row, const int32_t *__restrict__ grp_aux,
+    const int32_t *__restrict__ fib_idx, const int32_t *__restrict__ fib_ptr,
+    const int32_t *__restrict__ e_idx, const double *__restrict__ e_val,
+    const double *__restrict__ UF, int RF, const double *__restrict__ UE, int RE,
+    double *__restrict__ Yc, double *__restrict__ Ypart, int *__restrict__ next_task) {
     using S = FbStage<TF, TE>;
     constexpr int TR = FLO ? TE : TF, TC = FLO ? TF : TE;
     extern __shared__ __align__(16) unsigned char fb_smem[];
@@ -344,6 +348,17 @@ __global__ void __launch_bounds__(256, 2) ttmc3f_kernel(
     for (int j = 0; j < TF; j++) okF[j] = g + 8 * j < RF;
 #pragma unroll
     for (int j = 0; j < TE; j++) okE[j] = g + 8 * j < RE;
+    // This lane's two output entries of tile (r, c) in a row: p = pl + Rlo ph
+    // (-1: outside the row).
+    int off[TR][TC];
+#pragma unroll
+    for (int r = 0; r < TR; r++)
+#pragma unroll
+        for (int c = 0; c < TC; c++) {
+            const int ph = 8 * r + g, pl = 8 * c + 2 * t4;
+            off[r][c] = (ph < Rhi && pl < Rlo) ? pl + Rlo * ph : -1;
+        }
+    const bool pair = (Rlo & 1) == 0;
 
     auto ue_of = [&](int buf) { return reinterpret_cast<double *>(wsm + buf * S::BYTES); };
     auto uf_of = [&](int buf) { return ue_of(buf) + FB_NZ * S::PE; };
@@ -359,7 +374,10 @@ __global__ void __launch_bounds__(256, 2) ttmc3f_kernel(
         vv[lane] = m.v;
         if (lane < 4 * m.ng) fo[lane] = m.fofs;
         if (lane == 0) fo[4 * m.ng] = m.nzn;
-        if (lane <= m.ng) gr[lane] = m.grow;
+        if (lane < m.ng) {
+            gr[lane] = m.grow;
+            gr[FB_GRP + lane] = m.gaux;
+        }
         fb_stage_rows<8 * TE>(ue_of(buf), pe, UE, RE, m.nzn, m.idx, lane);
         fb_stage_rows<8 * TF>(uf_of(buf), pf, UF, RF, 4 * m.ng, m.fidx, lane);
         sp_cp_commit();
@@ -377,17 +395,19 @@ __global__ void __launch_bounds__(256, 2) ttmc3f_kernel(
         const int4 task = tasks[tk];
         const int b0 = task.x, b1 = task.y, slot = task.z;
         FbMeta m;
-        fb_load_meta(m, b0, lane, bt, grp_row, fib_idx, fib_ptr, e_idx, e_val);
+        fb_load_meta(m, b0, lane, bt, grp_row, grp_aux, fib_idx, fib_ptr, e_idx, e_val);
         stage(m, 0);
         int ng_cur = m.ng, ng_next = 0;
-        if (b0 + 1 < b1) fb_load_meta(m, b0 + 1, lane, bt, grp_row, fib_idx, fib_ptr, e_idx, e_val);
+        if (b0 + 1 < b1)
+            fb_load_meta(m, b0 + 1, lane, bt, grp_row, grp_aux, fib_idx, fib_ptr, e_idx, e_val);
         for (int b = b0; b < b1; b++) {
             const int buf = (b - b0) & 1;
             if (b + 1 < b1) {
                 stage(m, buf ^ 1);
                 ng_next = m.ng;
                 if (b + 2 < b1)
-                    fb_load_meta(m, b + 2, lane, bt, grp_row, fib_idx, fib_ptr, e_idx, e_val);
+                    fb_load_meta(m, b + 2, lane, bt, grp_row, grp_aux, fib_idx, fib_ptr, e_idx,
+                                 e_val);
                 sp_cp_wait<1>();
             } else {
                 sp_cp_wait<0>();
@@ -396,21 +416,23 @@ __global__ void __launch_bounds__(256, 2) ttmc3f_kernel(
             const double *ue = ue_of(buf), *uf = uf_of(buf), *vv = vv_of(buf);
             const int *fo = fo_of(buf);
             const int *gr = fo + FB_SLOTS + 1;
-            for (int j = 0; j < ng_cur; j++) {
+#pragma unroll
+            for (int j = 0; j < FB_GRP; j++) {
+                if (j >= ng_cur) break;
                 const int s = 4 * j + t4;
                 const int beg = fo[s], len = fo[s + 1] - beg;
-                int mx = max(len, __shfl_xor_sync(0xffffffffu, len, 1));
-                mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, 2));
+                const int aux = gr[FB_GRP + j];
+                const int mx = aux & (FB_ROW_END - 1);
                 double w[TE];
 #pragma unroll
                 for (int k = 0; k < TE; k++) w[k] = 0.0;
                 for (int q = 0; q < mx; q++) {
                     if (q < len) {
                         const double v = vv[beg + q];
-                        const double *row = ue + (beg + q) * pe + g;
+                        const double *rw = ue + (beg + q) * pe + g;
 #pragma unroll
                         for (int k = 0; k < TE; k++)
-                            if (okE[k]) w[k] = fma(v, row[8 * k], w[k]);
+                            if (okE[k]) w[k] = fma(v, rw[8 * k], w[k]);
                     }
                 }
                 double u[TF];
@@ -421,28 +443,24 @@ __global__ void __launch_bounds__(256, 2) ttmc3f_kernel(
 #pragma unroll
                     for (int c = 0; c < TC; c++)
                         sp_dmma(acc[r][c][0], acc[r][c][1], FLO ? w[r] : u[r], FLO ? u[c] : w[c]);
-                const int row = gr[j];
-                if (gr[j + 1] != row || (b == b1 - 1 && j == ng_cur - 1)) {
-                    double *dst = slot >= 0 ? Ypart + (int64_t)slot * P : Yc + (int64_t)row * P;
+                if ((aux & FB_ROW_END) || (b == b1 - 1 && j == ng_cur - 1)) {
+                    double *dst = slot >= 0 ? Ypart + (int64_t)slot * P : Yc + (int64_t)gr[j] * P;
 #pragma unroll
-                    for (int r = 0; r < TR; r++) {
-                        const int ph = 8 * r + g;
+                    for (int r = 0; r < TR; r++)
 #pragma unroll
                         for (int c = 0; c < TC; c++) {
-                            const int pl = 8 * c + 2 * t4;
-                            if (ph < Rhi) {
-                                double *d = dst + pl + (int64_t)Rlo * ph;
-                                if ((Rlo & 1) == 0 && pl + 1 < Rlo) {
-                                    *reinterpret_cast<double2 *>(d) =
+                            const int o = off[r][c];
+                            if (o >= 0) {
+                                if (pair) {
+                                    *reinterpret_cast<double2 *>(dst + o) =
                                         make_double2(acc[r][c][0], acc[r][c][1]);
                                 } else {
-                                    if (pl < Rlo) d[0] = acc[r][c][0];
-                                    if (pl + 1 < Rlo) d[1] = acc[r][c][1];
+                                    dst[o] = acc[r][c][0];
+                                    if (8 * c + 2 * t4 + 1 < Rlo) dst[o + 1] = acc[r][c][1];
                                 }
                             }
                             acc[r][c][0] = acc[r][c][1] = 0.0;
                         }
-                    }
                 }
             }
             __syncwarp();
@@ -460,10 +478,11 @@ __global__ void __launch_bounds__(256, 2) ttmc3f_kernel(
 template <int PL, bool FLO>
 __global__ void __launch_bounds__(256) ttmc3f_wide_kernel(
     const int4 *__restrict__ tasks, int64_t ntasks, const int2 *__restrict__ bt,
-    const int32_t *__restrict__ grp_row, const int32_t *__restrict__ fib_idx,
-    const int32_t *__restrict__ fib_ptr, const int32_t *__restrict__ e_idx,
-    const double *__restrict__ e_val, const double *__restrict__ UF, int RF,
-    const double *__restrict__ UE, int RE, double *__restrict__ Yc, double *__restrict__ Ypart) {
+    const int32_t *__restrict__ grp_row, const int32_t *__restrict__ grp_aux,
+    const int32_t *__restrict__ fib_idx, const int32_t *__restrict__ fib_ptr,
+    const int32_t *__restrict__ e_idx, const double *__restrict__ e_val,
+    const double *__restrict__ UF, int RF, const double *__restrict__ UE, int RE,
+    double *__restrict__ Yc, double *__restrict__ Ypart) {
     const int lane = threadIdx.x & 31;
     const int64_t gw = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -500,9 +519,8 @@ __global__ void __launch_bounds__(256) ttmc3f_wide_kernel(
 #pragma unroll
                 for (int q = 0; q < PL; q++) acc[q] = fma(__ldg(u + pF[q]), w[q], acc[q]);
             }
-            const int row = grp_row[gq];
-            if (grp_row[gq + 1] != row || gq == gend - 1) {
-                double *dst = slot >= 0 ? Ypart + (int64_t)slot * P : Yc + (int64_t)row * P;
+            if ((grp_aux[gq] & FB_ROW_END) || gq == gend - 1) {
+                double *dst = slot >= 0 ? Ypart + (int64_t)slot * P : Yc + (int64_t)grp_row[gq] * P;
 #pragma unroll
                 for (int q = 0; q < PL; q++) {
                     if (lane + 32 * q < P) dst[lane + 32 * q] = acc[q];
@@ -883,7 +901,7 @@ void build_mode_fibre(dt_ctx *ctx, dt_sptensor *sp, int n, const std::vector<Dev
         int64_t beg;
         int32_t len, idx;
     };
-    std::vector<int32_t> rows, row_grp, grp_row, fib_idx, fib_ptr, order;
+    std::vector<int32_t> rows, row_grp, grp_row, grp_aux, fib_idx, fib_ptr, order;
     fib_idx.reserve((size_t)best_fib * 5 / 4 + 16);
     fib_ptr.reserve((size_t)best_fib * 5 / 4 + 17);
     order.reserve((size_t)nnz);
@@ -911,11 +929,15 @@ void build_mode_fibre(dt_ctx *ctx, dt_sptensor *sp, int n, const std::vector<Dev
             fib_ptr.push_back((int32_t)order.size());
             for (int32_t j = 0; j < f.len; j++) order.push_back(best_ids[f.beg + j]);
         }
-        for (size_t q = 0; q < rf.size() / 4; q++) grp_row.push_back(k);
+        for (size_t q = 0; q < rf.size() / 4; q++) {
+            grp_row.push_back(k);
+            int32_t mx = 0;
+            for (int t = 0; t < 4; t++) mx = std::max(mx, rf[4 * q + t].len);
+            grp_aux.push_back(mx | (q + 1 == rf.size() / 4 ? FB_ROW_END : 0));
+        }
     }
     const int32_t ngroups = (int32_t)(fib_idx.size() / 4);
     row_grp.push_back(ngroups);
-    grp_row.push_back(-1);
     fib_ptr.push_back((int32_t)order.size());
     best_key.clear();
     best_key.shrink_to_fit();
@@ -1000,6 +1022,7 @@ void build_mode_fibre(dt_ctx *ctx, dt_sptensor *sp, int n, const std::vector<Dev
               mc.e_val.as<double>());
     upload(ctx, mc.rows, rows);
     upload(ctx, mc.grp_row, grp_row);
+    upload(ctx, mc.grp_aux, grp_aux);
     upload(ctx, mc.fib_idx, fib_idx);
     upload(ctx, mc.fib_ptr, fib_ptr);
     upload(ctx, mc.batches, bt);
@@ -1049,9 +1072,9 @@ void launch_fib(dt_ctx *ctx, const ModeCopy &mc, const double *UF, int RF, const
     DevMem next(ctx, sizeof(int));
     DT_CUDA(cudaMemsetAsync(next.get(), 0, sizeof(int), ctx->stream));
     DT_LAUNCH(ctx, kern, blocks, warps * 32, smem, mc.tasks.as<int4>(), mc.ntasks,
-              mc.batches.as<int2>(), mc.grp_row.as<int32_t>(), mc.fib_idx.as<int32_t>(),
-              mc.fib_ptr.as<int32_t>(), mc.e_idx.as<int32_t>(), mc.e_val.as<double>(), UF, RF,
-              UE, RE, Yc, Ypart, next.as<int>());
+              mc.batches.as<int2>(), mc.grp_row.as<int32_t>(), mc.grp_aux.as<int32_t>(),
+              mc.fib_idx.as<int32_t>(), mc.fib_ptr.as<int32_t>(), mc.e_idx.as<int32_t>(),
+              mc.e_val.as<double>(), UF, RF, UE, RE, Yc, Ypart, next.as<int>());
 }
 
 template <int PL, bool FLO>
@@ -1061,8 +1084,9 @@ void launch_fib_wide(dt_ctx *ctx, const ModeCopy &mc, const double *UF, int RF, 
     const unsigned blocks = (unsigned)std::max<int64_t>(
         1, std::min<int64_t>((mc.ntasks + 7) / 8, (int64_t)8 * ctx->num_sms));
     DT_LAUNCH(ctx, kern, blocks, 256, 0, mc.tasks.as<int4>(), mc.ntasks, mc.batches.as<int2>(),
-              mc.grp_row.as<int32_t>(), mc.fib_idx.as<int32_t>(), mc.fib_ptr.as<int32_t>(),
-              mc.e_idx.as<int32_t>(), mc.e_val.as<double>(), UF, RF, UE, RE, Yc, Ypart);
+              mc.grp_row.as<int32_t>(), mc.grp_aux.as<int32_t>(), mc.fib_idx.as<int32_t>(),
+              mc.fib_ptr.as<int32_t>(), mc.e_idx.as<int32_t>(), mc.e_val.as<double>(), UF, RF,
+              UE, RE, Yc, Ypart);
 }
 
 template <int TF, bool FLO>

@@ -452,31 +452,31 @@ __global__ void split_f32_kernel(const float *__restrict__ x, int64_t n,
 }
 
 // Sweep core from the K-major leaf rows: G[k + K*r] = sum_i Y[i][k] U[i][r]
-// (FP32 accumulate), one thread per (k, r); per-block partial sum of G^2 in
-// FP64.
+// in FP64 (hi + lo converts exactly), one thread per (k, r); per-block partial
+// sum of G^2 in FP64.
 __global__ void __launch_bounds__(256) core_rows_kernel(const __nv_bfloat16 *__restrict__ Yh,
                                                         const __nv_bfloat16 *__restrict__ Yl,
                                                         int64_t I, int64_t K,
                                                         const double *__restrict__ U, int R,
                                                         double *__restrict__ G,
                                                         double *__restrict__ part) {
-    extern __shared__ float Us[];  // I x R
-    for (int64_t e = threadIdx.x; e < I * R; e += blockDim.x) Us[e] = (float)U[e];
+    extern __shared__ double Us[];  // I x R
+    for (int64_t e = threadIdx.x; e < I * R; e += blockDim.x) Us[e] = U[e];
     __syncthreads();
     double s2 = 0.0;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < K * R;
          e += (int64_t)gridDim.x * blockDim.x) {
         const int64_t k = e % K;
         const int r = (int)(e / K);
-        const float *u = Us + (int64_t)I * r;
-        float acc = 0.f;
+        const double *u = Us + (int64_t)I * r;
+        double acc = 0.0;
         for (int64_t i = 0; i < I; i++) {
-            float y = __bfloat162float(Yh[i * K + k]);
-            if (Yl) y += __bfloat162float(Yl[i * K + k]);
-            acc = fmaf(y, u[i], acc);
+            double y = (double)__bfloat162float(Yh[i * K + k]);
+            if (Yl) y += (double)__bfloat162float(Yl[i * K + k]);
+            acc = fma(y, u[i], acc);
         }
         G[k + K * r] = acc;
-        s2 = fma((double)acc, (double)acc, s2);
+        s2 = fma(acc, acc, s2);
     }
     __shared__ double red[32];
     for (int o = 16; o > 0; o >>= 1) s2 += __shfl_down_sync(0xffffffffu, s2, o);
@@ -679,7 +679,9 @@ void core_rows(dt_ctx *ctx, const __nv_bfloat16 *Yh, const __nv_bfloat16 *Yl, in
     DT_CHECK_ARG(R <= 32, "core_rows: R %lld > 32", (long long)R);
     const int blocks = std::max(1, std::min<int>(4 * ctx->num_sms, (int)ceil_div(K * R, 256)));
     DevMem part(ctx, (size_t)blocks * sizeof(double));
-    DT_LAUNCH(ctx, core_rows_kernel, blocks, 256, I * R * sizeof(float), Yh, Yl, I, K, U, (int)R,
+    const size_t smem = (size_t)I * R * sizeof(double);
+    smem_limit(ctx, core_rows_kernel, smem);
+    DT_LAUNCH(ctx, core_rows_kernel, blocks, 256, smem, Yh, Yl, I, K, U, (int)R,
               G, part.as<double>());
     DT_LAUNCH(ctx, sum_double_kernel, 1, 1024, 0, part.as<double>(), blocks, g2_out);
 }

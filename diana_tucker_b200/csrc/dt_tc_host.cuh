@@ -64,7 +64,7 @@ void tc_gram(dt_ctx *ctx, const __nv_bfloat16 *Yh, const __nv_bfloat16 *Yl, int6
 void split_f32(dt_ctx *ctx, const float *x, int64_t n, __nv_bfloat16 *hi, __nv_bfloat16 *lo,
                double *sumsq_out);
 
-// G[k + K*r] = sum_i Y[i*K + k] U[i + I*r] (FP32 accumulate), ||G||^2 -> g2_out.
+// G[k + K*r] = sum_i Y[i*K + k] U[i + I*r] (FP64 accumulate), ||G||^2 -> g2_out.
 void core_rows(dt_ctx *ctx, const __nv_bfloat16 *Yh, const __nv_bfloat16 *Yl, int64_t I, int64_t K,
                const double *U, int64_t R, double *G, double *g2_out);
 
