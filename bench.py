@@ -42,6 +42,10 @@ RANKS = (16, 16, 16, 16)
 SHAPE = (96, 96, 96, 96)
 TARGET = 1e-6
 FALLBACK_HBM_GBS = 6650.0
+# Subspace-iteration steps per mode: the FP64 drop-in keeps the reference's
+# ALS_ (five); the mixed method uses two (its sweep count is unchanged here).
+FP64_INNER = 5
+MIXED_INNER = 2
 
 
 def _log(msg):
@@ -67,8 +71,14 @@ def _oracle_residual():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region: NVML
+    polled every ~2 ms from a thread (a timed region of a few ms still gets
+    samples), else nvidia-smi at 200 ms.  Reads only; changes no setting."""
 
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -77,8 +87,25 @@ class ClockSampler:
         self.device = device
         self.proc = None
         self.lines = []
+        self.samples = []
+        self.reasons = set()
+        self.max_mhz = None
+        self.nvml = None
+        self.stop_ev = threading.Event()
+        self.t = None
 
     def start(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(self.device)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.nvml = (nv, h)
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
@@ -89,11 +116,37 @@ class ClockSampler:
         except Exception:
             self.proc = None
 
+    def _poll(self):
+        nv, h = self.nvml
+        while True:
+            try:
+                self.samples.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                mask = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                for name, const in self.REASONS:
+                    if mask & getattr(nv, const):
+                        self.reasons.add(name)
+            except Exception:
+                return
+            if self.stop_ev.wait(0.002):
+                return
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nvml is not None:
+            self.stop_ev.set()
+            self.t.join(timeout=5)
+            try:
+                self.nvml[0].nvmlShutdown()
+            except Exception:
+                pass
+            if not self.samples:
+                return None
+            sm = sorted(self.samples)
+            return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": self.max_mhz,
+                    "reasons": sorted(self.reasons), "samples": len(sm), "source": "nvml"}
         if not self.proc:
             return None
         self.proc.terminate()
@@ -119,7 +172,7 @@ class ClockSampler:
             return None
         sm.sort()
         return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi"}
 
 
 def _dist_setup(n_gpus):
@@ -175,15 +228,19 @@ def run_ours(args):
     X = datasets.dense_96x4_fp32()
     flat = np.ascontiguousarray(X.reshape(-1, order="F"))
     Xd = torch.from_numpy(flat).to(f"cuda:{local}")
-    kw = dict(init="randn", seed=1, max_sweeps=30, tol=1e-9, inner_iters=5, shape=SHAPE)
+    kw = dict(init="randn", seed=1, max_sweeps=30, tol=1e-9, shape=SHAPE)
 
     X64d = Xd.double()  # the FP64 drop-in takes Tensor<double>
 
+    # Inputs and outputs stay in HBM for `value` (G and U come back as CUDA
+    # tensors); `e2e` below copies them from and to the host.
     def mixed(profile=False):
-        return ctx.hooi_dense(Xd, RANKS, precision=DT_PREC_BF16X2, profile=profile, **kw)
+        return ctx.hooi_dense(Xd, RANKS, precision=DT_PREC_BF16X2, profile=profile,
+                              inner_iters=MIXED_INNER, device_out=True, **kw)
 
-    def fp64(profile=False, x=X64d):
-        return ctx.hooi_dense(x, RANKS, precision=DT_PREC_FP64, profile=profile, **kw)
+    def fp64(profile=False, x=X64d, inner=FP64_INNER):
+        return ctx.hooi_dense(x, RANKS, precision=DT_PREC_FP64, profile=profile,
+                              inner_iters=inner, device_out=True, **kw)
 
     # Warm-up (module loading, memory pool).
     _log("warm-up")
@@ -233,6 +290,7 @@ def run_ours(args):
     n64 = max(1, min(args.steps, 3))
     fp64_ms, r64 = bracket(fp64, n64)
     fp64_x32_ms, _ = bracket(lambda: fp64(x=Xd), n64)
+    fp64_in2_ms, r64b = bracket(lambda: fp64(inner=MIXED_INNER), n64)
     del X64d
 
     _log("end to end from pinned host memory")
@@ -241,7 +299,8 @@ def run_ours(args):
     e2e_t = []
     for i in range(max(1, min(args.steps, 3)) + 1):
         t0 = time.perf_counter()
-        G, U, _ = ctx.hooi_dense(Xh, RANKS, precision=DT_PREC_BF16X2, **kw)
+        G, U, _ = ctx.hooi_dense(Xh, RANKS, precision=DT_PREC_BF16X2, inner_iters=MIXED_INNER,
+                                 **kw)
         dt = (time.perf_counter() - t0) * 1e3
         if i > 0:
             e2e_t.append(dt)
@@ -280,12 +339,16 @@ def run_ours(args):
         "config": {
             "workload": "dense 96x96x96x96 FP32 Tucker(16^4, core*0.9^(i+j+k+l)) + N(0,1e-6), "
                         "seed 1; HOOI ranks 16^4; BF16 tcgen05 TTM chain + Gram with split "
-                        "hi/lo refinement, FP64 subspace iteration / fit / final core",
+                        "hi/lo operands, FP64 subspace iteration (2 steps per mode) / fit / "
+                        "final core projected from X",
             "init": "libc-seeded Gaussian + QR (seed 1)",
             "stop": "split hi+lo BF16 sweeps until the residual changes by < 5e-6 "
                     "(the split-precision noise floor); then the FP64 core projection",
             "target": f"|rel-err - FP64 oracle rel-err| <= {TARGET}",
             "l2": "inputs larger than L2 (X: 340 MB FP32, 170 MB per BF16 half; L2 126 MB)",
+            "outputs": "G and U stay in HBM (CUDA tensors); e2e copies them to the host",
+            "plans": "repeated calls reuse the context's cached plan and captured sweep "
+                     "graphs (built in warm-up), for both the mixed and the FP64 path",
             "parallelism": f"replicas x{world} (no data-path collective)",
         },
         "rel_err": rep["residual"],
@@ -296,8 +359,13 @@ def run_ours(args):
         "fp64_gpu": {"ms": round(fp64_ms, 4), "rel_err": r64["residual"], "sweeps": r64["sweeps"],
                      "x_dtype": "f64",
                      "speedup_mixed_vs_fp64": round(fp64_ms / ms, 3) if ms > 0 else None,
+                     "inner_iters": FP64_INNER,
                      "ms_x_f32": round(fp64_x32_ms, 4),
-                     "speedup_mixed_vs_fp64_x_f32": round(fp64_x32_ms / ms, 3) if ms > 0 else None},
+                     "speedup_mixed_vs_fp64_x_f32": round(fp64_x32_ms / ms, 3) if ms > 0 else None,
+                     "ms_inner_iters_2": round(fp64_in2_ms, 4),
+                     "sweeps_inner_iters_2": r64b["sweeps"],
+                     "speedup_mixed_vs_fp64_inner_iters_2":
+                         round(fp64_in2_ms / ms, 3) if ms > 0 else None},
         "decompositions_per_s": round(world * 1000.0 / ms, 3) if ms > 0 else None,
         "e2e": {"value": round(e2e_ms, 4), "unit": "ms", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
@@ -349,16 +417,31 @@ def _ttmc(ctx, peak, draws=50_000_000):
     sp.hooi(R, 1, Ut)
     _, _, rep = sp.hooi(R, 1, Ut)
     gbs = rep["ttm_x_bytes"] / (rep["ttm_x_ms"] * 1e-3) / 1e9 if rep["ttm_x_ms"] else 0.0
-    # Every nonzero also gathers one row of each other factor (2 x 16 doubles):
-    # traffic the unblocked TTMc must move through L2 (and from HBM for the
-    # 2e6-row factor, which exceeds L2), outside the algorithmic bytes above.
-    gather = float(len(vals)) * 3 * (2 * 16 * 8)
+    # The same launches against the per-mode figure of the COO format the
+    # reference reads (int64 indices + FP64 value = 32 B per nonzero, each other
+    # factor once, the non-empty Y_(n) rows written): nnz*32 + sum_{m!=n} I_m R_m 8
+    # + rows_n * P * 8, summed over the 3 modes.
+    import numpy as np
+    rows = [int(np.unique(i).size) for i in idx]
+    coo = 0.0
+    for n in range(3):
+        coo += len(vals) * 32.0 + rows[n] * 256 * 8.0
+        coo += sum(shape[m] * R[m] * 8.0 for m in range(3) if m != n)
+    coo_gbs = coo / (rep["ttm_x_ms"] * 1e-3) / 1e9 if rep["ttm_x_ms"] else 0.0
+    # Every nonzero also gathers one 128-byte row of its element-mode factor
+    # (and every fibre one of its fibre-mode factor) through L2: a lower bound
+    # of that traffic is nnz * 128 B per mode.
+    gather = float(len(vals)) * 3 * (16 * 8)
     eff = (rep["ttm_x_bytes"] + gather) / (rep["ttm_x_ms"] * 1e-3) / 1e9 if rep["ttm_x_ms"] else 0.0
     sp.close()
     return {"value": round(gbs, 1), "unit": "GB/s", "frac_of_hbm": round(gbs / peak, 4),
-            "nnz": int(len(vals)), "launches": rep["ttm_x_launches"],
+            "bytes_def": "fibre layout read (12 B/nonzero + 8 B/fibre slot) + Y rows written "
+                         "+ factors",
+            "nnz": int(len(vals)), "rows_per_mode": rows, "launches": rep["ttm_x_launches"],
             "ms": rep["ttm_x_ms"], "bytes": rep["ttm_x_bytes"],
-            "gather_bytes": gather, "with_gathers_gbs": round(eff, 1),
+            "coo_bytes": coo, "coo_gbs": round(coo_gbs, 1),
+            "coo_frac_of_hbm": round(coo_gbs / peak, 4),
+            "gather_bytes_lower_bound": gather, "with_gathers_gbs": round(eff, 1),
             "sweep_ms": rep["device_ms"], "gen_s": round(gen_s, 1)}
 
 

@@ -251,9 +251,12 @@ class Context:
     # -- dense HOOI ----------------------------------------------------------
     def hooi_dense(self, X, ranks, *, init="randn", seed=1, U0=None, max_sweeps=5, tol=0.0,
                    inner_iters=5, precision=DT_PREC_FP64, refine_sweeps=0, verbose=False,
-                   want_factors=True, want_core=True, profile=False, shape=None):
+                   want_factors=True, want_core=True, profile=False, shape=None,
+                   device_out=False):
         """Algorithm::Tucker::HOOI_ALS.  X: numpy or torch (float64/float32),
-        column-major.  Returns (G, U, report-dict)."""
+        column-major.  Returns (G, U, report-dict); with device_out and a CUDA
+        torch X, G and U are float64 CUDA tensors with column-major strides
+        (no copy back to the host), else numpy arrays."""
         self._bind(X)
         is_torch = _is_torch(X)
         if is_torch:
@@ -285,19 +288,34 @@ class Context:
         opts.refine_sweeps = refine_sweeps
         opts.verbose = int(verbose)
         opts.profile = int(profile)
-        G = np.zeros(ranks, order="F") if want_core else None
-        U = ([np.zeros((shape[n], ranks[n]), order="F") for n in range(N)]
-             if (want_factors or U0 is not None) else None)
-        if U0 is not None:
-            for n in range(N):
-                U[n][...] = np.asarray(U0[n], dtype=np.float64)
-        Uptr = (ctypes.c_void_p * N)(*[u.ctypes.data for u in U]) if U is not None else None
+        on_device = bool(device_out and is_torch and X.is_cuda)
+        if on_device:
+            import torch
+            dev = X.device
+            # Column-major buffers: allocate the reversed shape row-major and
+            # permute back.
+            G = (torch.zeros(ranks[::-1], dtype=torch.float64, device=dev)
+                 .permute(*range(N - 1, -1, -1)) if want_core else None)
+            U = ([torch.zeros((ranks[n], shape[n]), dtype=torch.float64, device=dev).t()
+                  for n in range(N)] if (want_factors or U0 is not None) else None)
+            if U0 is not None:
+                for n in range(N):
+                    U[n].copy_(torch.as_tensor(np.asarray(U0[n], dtype=np.float64)))
+            gptr = ctypes.c_void_p(G.data_ptr()) if G is not None else None
+            Uptr = (ctypes.c_void_p * N)(*[u.data_ptr() for u in U]) if U is not None else None
+        else:
+            G = np.zeros(ranks, order="F") if want_core else None
+            U = ([np.zeros((shape[n], ranks[n]), order="F") for n in range(N)]
+                 if (want_factors or U0 is not None) else None)
+            if U0 is not None:
+                for n in range(N):
+                    U[n][...] = np.asarray(U0[n], dtype=np.float64)
+            gptr = ctypes.c_void_p(G.ctypes.data) if G is not None else None
+            Uptr = (ctypes.c_void_p * N)(*[u.ctypes.data for u in U]) if U is not None else None
         rep = HooiReport()
         s, r = _shape_arr(shape), _shape_arr(ranks)
         _lib.check(self.lib.dt_hooi_dense(self.h, xptr, dtype, N, _i64p(s), _i64p(r),
-                                          ctypes.byref(opts),
-                                          ctypes.c_void_p(G.ctypes.data) if G is not None else None,
-                                          Uptr, ctypes.byref(rep)))
+                                          ctypes.byref(opts), gptr, Uptr, ctypes.byref(rep)))
         return G, U, rep.as_dict()
 
     # -- learned warm start ------------------------------------------------------

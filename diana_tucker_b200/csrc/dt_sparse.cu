@@ -225,18 +225,20 @@ constexpr int FB_GRP = 4;
 constexpr int FB_SLOTS = 4 * FB_GRP;
 constexpr int FB_ROW_END = 1 << 8;  // grp_aux: the group is the last of its row
 
-// Shared row pitch (doubles) for a staged factor row of R entries: even (16-byte
-// pieces) and 4 mod 8, so four rows read by one fragment load start in
-// different banks.
-__host__ __device__ constexpr int fb_pitch(int R) {
-    int p = (R + 1) & ~1;
-    while (p % 8 != 4) p += 2;
-    return p;
+// A staged factor row of up to 8 T entries has a pitch of 8 T doubles.  Four
+// rows read by one fragment load (8 consecutive doubles each) start in the
+// same bank when the pitch is 16 or 32 doubles, so column c of row j is stored
+// at c ^ fb_swz(j): rows alternate between the two 64-byte halves of a bank
+// cycle (pitch 16) or its four 64-byte quarters (pitch 32).  Pitches 8 and 24
+// alternate by themselves.
+__host__ __device__ constexpr int fb_pitch(int T) { return 8 * T; }
+__device__ __forceinline__ int fb_swz(int row, int pitch) {
+    return pitch == 16 ? (row & 1) << 3 : pitch == 32 ? (row & 3) << 3 : 0;
 }
 
 template <int TF, int TE>
 struct FbStage {
-    static constexpr int PE = fb_pitch(8 * TE), PF = fb_pitch(8 * TF);
+    static constexpr int PE = fb_pitch(TE), PF = fb_pitch(TF);
     static constexpr int DOUBLES = FB_NZ * PE + FB_SLOTS * PF + FB_NZ;
     static constexpr int INTS = FB_SLOTS + 1 + 2 * FB_GRP;
     static constexpr int BYTES = DOUBLES * 8 + ((INTS * 4 + 15) & ~15);
@@ -297,12 +299,14 @@ __host__ __device__ constexpr int fb_pow2(int x) {
 }
 
 // Copies n <= 32 rows of the transposed factor U (R <= RMAX doubles each; the
-// index of row j is held by lane j) into dst rows of `pitch` doubles.  Lane l
-// copies piece l % PPR of row l / PPR (+ 32 / PPR per step), PPR a power of
-// two: 16-byte pieces when R is even and U 16-byte aligned, else 8-byte ones.
+// index of row j is held by lane j) into dst rows of RMAX doubles, swizzled
+// (fb_swz).  Lane l copies piece l % PPR of row l / PPR (+ 32 / PPR per step),
+// PPR a power of two: 16-byte pieces when R is even and U 16-byte aligned,
+// else 8-byte ones.
 template <int RMAX>
-__device__ __forceinline__ void fb_stage_rows(double *dst, int pitch, const double *__restrict__ U,
-                                              int R, int n, int ridx, int lane) {
+__device__ __forceinline__ void fb_stage_rows(double *dst, const double *__restrict__ U, int R,
+                                              int n, int ridx, int lane) {
+    constexpr int pitch = RMAX;
     if ((R & 1) == 0 && (reinterpret_cast<uintptr_t>(U) & 15) == 0) {
         constexpr int PPR = fb_pow2(RMAX / 2), RPI = 32 / PPR;
         const int rem = lane % PPR, jl = lane / PPR;
@@ -310,7 +314,9 @@ __device__ __forceinline__ void fb_stage_rows(double *dst, int pitch, const doub
         for (int j0 = 0; j0 < n; j0 += RPI) {
             const int j = j0 + jl;
             const int i = __shfl_sync(0xffffffffu, ridx, j & 31);
-            if (j < n && okp) sp_cp16(dst + j * pitch + 2 * rem, U + (int64_t)i * R + 2 * rem);
+            if (j < n && okp)
+                sp_cp16(dst + j * pitch + ((2 * rem) ^ fb_swz(j, pitch)),
+                        U + (int64_t)i * R + 2 * rem);
         }
     } else {
         constexpr int PPR = fb_pow2(RMAX), RPI = 32 / PPR;
@@ -319,7 +325,8 @@ __device__ __forceinline__ void fb_stage_rows(double *dst, int pitch, const doub
         for (int j0 = 0; j0 < n; j0 += RPI) {
             const int j = j0 + jl;
             const int i = __shfl_sync(0xffffffffu, ridx, j & 31);
-            if (j < n && okp) sp_cp8(dst + j * pitch + rem, U + (int64_t)i * R + rem);
+            if (j < n && okp)
+                sp_cp8(dst + j * pitch + (rem ^ fb_swz(j, pitch)), U + (int64_t)i * R + rem);
         }
     }
 }
@@ -342,7 +349,7 @@ __global__ void __launch_bounds__(256, 2) ttmc3f_kernel(
     const int64_t nw = (int64_t)gridDim.x * nwarp_blk;
     const int P = RF * RE;
     const int Rlo = FLO ? RF : RE, Rhi = FLO ? RE : RF;
-    const int pe = fb_pitch(RE), pf = fb_pitch(RF);
+    constexpr int pe = S::PE, pf = S::PF;
     bool okF[TF], okE[TE];
 #pragma unroll
     for (int j = 0; j < TF; j++) okF[j] = g + 8 * j < RF;
@@ -378,8 +385,8 @@ __global__ void __launch_bounds__(256, 2) ttmc3f_kernel(
             gr[lane] = m.grow;
             gr[FB_GRP + lane] = m.gaux;
         }
-        fb_stage_rows<8 * TE>(ue_of(buf), pe, UE, RE, m.nzn, m.idx, lane);
-        fb_stage_rows<8 * TF>(uf_of(buf), pf, UF, RF, 4 * m.ng, m.fidx, lane);
+        fb_stage_rows<8 * TE>(ue_of(buf), UE, RE, m.nzn, m.idx, lane);
+        fb_stage_rows<8 * TF>(uf_of(buf), UF, RF, 4 * m.ng, m.fidx, lane);
         sp_cp_commit();
     };
 
@@ -428,16 +435,20 @@ __global__ void __launch_bounds__(256, 2) ttmc3f_kernel(
                 for (int k = 0; k < TE; k++) w[k] = 0.0;
                 for (int q = 0; q < mx; q++) {
                     if (q < len) {
-                        const double v = vv[beg + q];
-                        const double *rw = ue + (beg + q) * pe + g;
+                        const int r = beg + q;
+                        const double v = vv[r];
+                        const double *rw = ue + r * pe;
+                        const int sw = fb_swz(r, pe);
 #pragma unroll
                         for (int k = 0; k < TE; k++)
-                            if (okE[k]) w[k] = fma(v, rw[8 * k], w[k]);
+                            if (okE[k]) w[k] = fma(v, rw[(g + 8 * k) ^ sw], w[k]);
                     }
                 }
                 double u[TF];
+                const int swf = fb_swz(s, pf);
 #pragma unroll
-                for (int k = 0; k < TF; k++) u[k] = (okF[k] && len > 0) ? uf[s * pf + g + 8 * k] : 0.0;
+                for (int k = 0; k < TF; k++)
+                    u[k] = (okF[k] && len > 0) ? uf[s * pf + ((g + 8 * k) ^ swf)] : 0.0;
 #pragma unroll
                 for (int r = 0; r < TR; r++)
 #pragma unroll
@@ -667,21 +678,31 @@ __global__ void __launch_bounds__(256) mtr_mma_kernel(const double *__restrict__
             __syncthreads();
             const int kn = (int)min((int64_t)KB, k1 - kb);
             const int ks_end = (kn + 3) / 4;
-            for (int ks = 0; ks < ks_end; ks++) {
-                const int bl = 4 * ks + t;
-                const int64_t k = kb + bl;
-                const bool okk = bl < kn;
-                double bv[NTL];
+            // Four k-steps of Yc loads are issued before their MMAs, so 4 MG
+            // loads per lane are in flight.
+            for (int ks0 = 0; ks0 < ks_end; ks0 += 4) {
+                double av[4][MG], bv[4][NTL];
 #pragma unroll
-                for (int j = 0; j < NTL; j++) bv[j] = Us[bl * LDU + 8 * j + g];
+                for (int u = 0; u < 4; u++) {
+                    const int bl = 4 * (ks0 + u) + t;
+                    const int64_t k = kb + bl;
+                    const bool okk = bl < kn;
 #pragma unroll
-                for (int m = 0; m < MG; m++) {
-                    const int mt = mbase + w + 8 * m;
-                    const int p = 8 * mt + g;
-                    const double a = (okk && mt < ptiles && p < P) ? Yc[k * P + p] : 0.0;
+                    for (int j = 0; j < NTL; j++) bv[u][j] = okk ? Us[bl * LDU + 8 * j + g] : 0.0;
 #pragma unroll
-                    for (int j = 0; j < NTL; j++) sp_dmma(acc[m][j][0], acc[m][j][1], a, bv[j]);
+                    for (int m = 0; m < MG; m++) {
+                        const int mt = mbase + w + 8 * m;
+                        const int p = 8 * mt + g;
+                        av[u][m] = (okk && mt < ptiles && p < P) ? Yc[k * P + p] : 0.0;
+                    }
                 }
+#pragma unroll
+                for (int u = 0; u < 4; u++)
+#pragma unroll
+                    for (int m = 0; m < MG; m++)
+#pragma unroll
+                        for (int j = 0; j < NTL; j++)
+                            sp_dmma(acc[m][j][0], acc[m][j][1], av[u][m], bv[u][j]);
             }
         }
 #pragma unroll
@@ -711,13 +732,31 @@ __global__ void scatter_rows_kernel(const double *__restrict__ Yc,
     }
 }
 
-__global__ void sum_blocks_kernel(const double *__restrict__ part, int nblk, int64_t n,
-                                  double *__restrict__ out) {
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
-         e += (int64_t)gridDim.x * blockDim.x) {
-        double s = 0.0;
-        for (int b = 0; b < nblk; b++) s += part[(int64_t)b * n + e];
-        out[e] = s;
+// out[e] = sum_b part[b * n + e]: 64 outputs per CTA, 4 threads per output
+// each summing every 4th block into 4 accumulators (16 loads in flight), then
+// a fixed-order add (deterministic).
+__global__ void __launch_bounds__(256) sum_blocks_kernel(const double *__restrict__ part,
+                                                         int nblk, int64_t n,
+                                                         double *__restrict__ out) {
+    __shared__ double red[4][64];
+    const int s = threadIdx.x >> 6, o = threadIdx.x & 63;
+    for (int64_t e0 = (int64_t)blockIdx.x * 64; e0 < n; e0 += (int64_t)gridDim.x * 64) {
+        const int64_t e = e0 + o;
+        double a[4] = {0.0, 0.0, 0.0, 0.0};
+        if (e < n) {
+            int b = s;
+            for (; b + 12 < nblk; b += 16) {
+#pragma unroll
+                for (int j = 0; j < 4; j++) a[j] += part[(int64_t)(b + 4 * j) * n + e];
+            }
+#pragma unroll
+            for (int j = 0; j < 3; j++)
+                if (b + 4 * j < nblk) a[j] += part[(int64_t)(b + 4 * j) * n + e];
+        }
+        red[s][o] = (a[0] + a[1]) + (a[2] + a[3]);
+        __syncthreads();
+        if (s == 0 && e < n) out[e] = (red[0][o] + red[1][o]) + (red[2][o] + red[3][o]);
+        __syncthreads();
     }
 }
 
@@ -1061,6 +1100,8 @@ void launch_fib(dt_ctx *ctx, const ModeCopy &mc, const double *UF, int RF, const
     // Two CTAs per SM when their stages fit in half of the 228 KB (1 KB of
     // each CTA's share is reserved), else one.
     int per_sm = 2, warps = std::min(8, (228 * 1024 / 2 - 1024) / S::WARP_BYTES);
+    // An even warp count per CTA spreads warps evenly over the 4 schedulers.
+    if (warps > 1 && warps < 8) warps &= ~1;
     if (warps < 1) {
         per_sm = 1;
         warps = std::max(1, std::min(8, (227 * 1024) / S::WARP_BYTES));
@@ -1213,8 +1254,8 @@ void sp_mtr(dt_ctx *ctx, const dt_sptensor *sp, const double *Yc, int mode, int 
     else DT_MTR(4);
 #undef DT_MTR
     const int64_t n = (int64_t)P * Rn;
-    DT_LAUNCH(ctx, sum_blocks_kernel, std::max(1u, ceil_div(n, 256)), 256, 0,
-              part.as<double>(), nblk, n, L);
+    DT_LAUNCH(ctx, sum_blocks_kernel, std::max(1u, std::min<unsigned>(ceil_div(n, 64), 65535)),
+              256, 0, part.as<double>(), nblk, n, L);
 }
 
 void sp_mtl(dt_ctx *ctx, const dt_sptensor *sp, const double *Yc, int mode, int P,
