@@ -12,6 +12,7 @@ The C++ drop-in for the reference's own API (``Tensor<Ty>``, ``SpTensor<Ty>``,
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 
@@ -421,9 +422,70 @@ class Context:
                   "tune_ms": list(rep.tune_ms)}
         return Uo, Go, relerr, report
 
+    # -- Summary profiler --------------------------------------------------------
+    def summary_enable(self, on: bool = True):
+        """Summary::init / finalize: record named, nested device-timed ranges."""
+        self._bind()
+        _lib.check(self.lib.dt_summary_enable(self.h, int(on)))
+
+    def summary_reset(self):
+        _lib.check(self.lib.dt_summary_reset(self.h))
+
+    def summary_table(self) -> str:
+        """Summary::print_summary's table of the recorded ranges (recording
+        restarts afterwards)."""
+        need = ctypes.c_int64()
+        buf = ctypes.create_string_buffer(1 << 22)
+        _lib.check(self.lib.dt_summary_table(self.h, buf, len(buf), ctypes.byref(need)))
+        return buf.value.decode()
+
     # -- sparse ----------------------------------------------------------------
     def sptensor(self, idx, vals, shape):
         return SpTensor(self, idx, vals, shape)
+
+    def _tns_handle(self, path=None, data=None):
+        self._bind()
+        h, nd, nz = ctypes.c_void_p(), ctypes.c_int(), ctypes.c_int64()
+        if path is not None:
+            _lib.check(self.lib.dt_tns_read(self.h, os.fsencode(path), ctypes.byref(h),
+                                            ctypes.byref(nd), ctypes.byref(nz)))
+        else:
+            buf = np.frombuffer(bytes(data), dtype=np.uint8)
+            _lib.check(self.lib.dt_tns_parse(self.h, buf.ctypes.data, buf.size, ctypes.byref(h),
+                                             ctypes.byref(nd), ctypes.byref(nz)))
+        return h, nd.value, nz.value
+
+    def read_tns(self, path=None, data=None):
+        """read_data<double> on the device (dt_tns_read / dt_tns_parse): a .tns
+        file by path, or its bytes.  Returns (idx: list of 0-based int64
+        arrays, vals, dims)."""
+        h, nd, nz = self._tns_handle(path, data)
+        try:
+            dims = np.zeros(nd, dtype=np.int64)
+            idx = [np.zeros(nz, dtype=np.int64) for _ in range(nd)]
+            vals = np.zeros(nz)
+            ptrs = (ctypes.c_void_p * nd)(*[i.ctypes.data for i in idx])
+            _lib.check(self.lib.dt_tns_copy(self.h, h, _i64p(dims), ptrs, vals.ctypes.data))
+        finally:
+            self.lib.dt_tns_destroy(h)
+        return idx, vals, dims
+
+    def sptensor_from_tns(self, path=None, data=None):
+        """The parsed file as a device-built SpTensor (dt_tns_to_sptensor), with
+        no host round trip of the nonzeros."""
+        h, nd, nz = self._tns_handle(path, data)
+        try:
+            dims = np.zeros(nd, dtype=np.int64)
+            _lib.check(self.lib.dt_tns_copy(self.h, h, _i64p(dims), None, None))
+            sp = SpTensor.__new__(SpTensor)
+            sp.ctx, sp.lib, sp.ndim, sp.nnz = self, self.lib, nd, nz
+            sp.shape = [int(d) for d in dims]
+            sh = ctypes.c_void_p()
+            _lib.check(self.lib.dt_tns_to_sptensor(self.h, h, ctypes.byref(sh)))
+            sp.h = sh
+        finally:
+            self.lib.dt_tns_destroy(h)
+        return sp
 
 
 class SpTensor:

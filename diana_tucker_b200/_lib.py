@@ -144,6 +144,17 @@ _SIGS = [
                                        _vp]),
     ("dt_sp_hooi", ctypes.c_int, [_vp, _vp, c_i64p, ctypes.c_int, ctypes.POINTER(_vp), _vp,
                                   ctypes.POINTER(HooiReport)]),
+    ("dt_tns_read", ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.POINTER(_vp),
+                                   ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int64)]),
+    ("dt_tns_parse", ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.POINTER(_vp),
+                                    ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int64)]),
+    ("dt_tns_copy", ctypes.c_int, [_vp, _vp, c_i64p, ctypes.POINTER(_vp), _vp]),
+    ("dt_tns_to_sptensor", ctypes.c_int, [_vp, _vp, ctypes.POINTER(_vp)]),
+    ("dt_tns_destroy", ctypes.c_int, [_vp]),
+    ("dt_summary_enable", ctypes.c_int, [_vp, ctypes.c_int]),
+    ("dt_summary_reset", ctypes.c_int, [_vp]),
+    ("dt_summary_table", ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_int64,
+                                        ctypes.POINTER(ctypes.c_int64)]),
 ]
 
 EXPORTED = [s[0] for s in _SIGS]

@@ -9,6 +9,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cstdlib>
 #include <vector>
 
 #include "tensor.hpp"
@@ -22,6 +23,35 @@ class data_buffer {
     Ty *vals = nullptr;
     size_t *dims = nullptr;
 };
+
+// read_data<double> (include/read_data.hpp:20-21, src/read_data.cpp:36-129):
+// parses the .tns file on the device (dt_tns_read) and fills dbf with
+// malloc'd arrays, 0-based size_t indices and dims = max index + 1, as the
+// reference does; SpTensor takes them over.
+template <typename Ty>
+void read_data(char *filename, data_buffer<Ty> *dbf);
+
+template <>
+inline void read_data<double>(char *filename, data_buffer<double> *dbf) {
+    dt_tns *t = nullptr;
+    int nd = 0;
+    int64_t nz = 0;
+    diana::check(dt_tns_read(diana::ctx(), filename, &t, &nd, &nz), "read_data");
+    dbf->ndim = (size_t)nd;
+    dbf->nnz = (size_t)nz;
+    dbf->dims = (size_t *)std::malloc(nd * sizeof(size_t));
+    dbf->index_lists = (size_t **)std::malloc(nd * sizeof(size_t *));
+    std::vector<int64_t *> idx(nd);
+    for (int m = 0; m < nd; m++) {
+        dbf->index_lists[m] = (size_t *)std::malloc(nz * sizeof(size_t));
+        idx[m] = reinterpret_cast<int64_t *>(dbf->index_lists[m]);
+    }
+    dbf->vals = (double *)std::malloc(nz * sizeof(double));
+    const int rc = dt_tns_copy(diana::ctx(), t, reinterpret_cast<int64_t *>(dbf->dims), idx.data(),
+                               dbf->vals);
+    dt_tns_destroy(t);
+    diana::check(rc, "read_data");
+}
 
 template <typename Ty>
 class SpTensor;

@@ -33,6 +33,8 @@ struct dt_ctx {
     // of one sweep), reused by the next call with the same shapes, ranks and
     // options; released before the stream at dt_ctx_destroy.
     std::shared_ptr<void> hooi_plan_fp64, hooi_plan_mixed;
+    // Summary profiler state (dt_summary_*; null until first enabled).
+    std::shared_ptr<void> summary;
 };
 
 namespace dt {
@@ -165,6 +167,21 @@ class SweepGraph {
     cudaGraphExec_t exec_ = nullptr;
     int64_t launches_ = 0;
     bool failed_ = false;
+};
+
+// A named range of the Summary profiler (dt_summary_enable): CUDA events on
+// ctx->stream around the scope, nested in the enclosing range, with the
+// operation's flop and byte counts.  Does nothing unless the profiler is on.
+// Not for use inside stream capture.
+class SummaryScope {
+   public:
+    SummaryScope(dt_ctx *ctx, const char *name, double flop = 0, double bytes = 0);
+    ~SummaryScope();
+    SummaryScope(const SummaryScope &) = delete;
+    SummaryScope &operator=(const SummaryScope &) = delete;
+
+   private:
+    dt_ctx *ctx_ = nullptr;
 };
 
 // Drops a cached HOOI plan once the work queued on ctx->stream is done.

@@ -201,6 +201,7 @@ int dt_ctx_destroy(dt_ctx *ctx) {
         if (ctx->stream) cudaStreamSynchronize(ctx->stream);
         ctx->hooi_plan_fp64.reset();
         ctx->hooi_plan_mixed.reset();
+        ctx->summary.reset();
         if (ctx->stream) cudaStreamSynchronize(ctx->stream);
         if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
         if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);

@@ -237,6 +237,25 @@ void DenseHooi::init_factors(double *const *U_user) {
     }
 }
 
+// The two passes over X of a sweep: each half of the dimension tree first
+// contracts X over its largest size reduction.
+double DenseHooi::x_pass_flop() const {
+    if (N == 1) return 2.0 * xsize * I[0];
+    double f = 0.0;
+    for (int side = 0; side < 2; side++) {
+        const int lo = side == 0 ? N / 2 : 0, hi = side == 0 ? N : N / 2;
+        int best = lo;
+        for (int m = lo; m < hi; m++)
+            if ((double)I[m] / R[m] > (double)I[best] / R[best]) best = m;
+        f += 2.0 * xsize * R[best];
+    }
+    return f;
+}
+
+double DenseHooi::x_pass_bytes() const {
+    return 2.0 * xsize * (dtype == DT_F64 ? 8 : 4);
+}
+
 double DenseHooi::read_scalar(int k) {
     double h = 0.0;
     DT_CUDA(cudaMemcpyAsync(&h, scal.as<double>() + k, sizeof(double), cudaMemcpyDeviceToHost,
@@ -257,10 +276,15 @@ void DenseHooi::run(double *G_user, double *const *U_user, dt_hooi_report *rep,
     double prev = -1.0, res = 0.0;
     int sweeps = 0;
     for (int it = 0; it < opts.max_sweeps; it++) {
-        if (graph && !opts.profile)
-            graph->run(ctx, [&] { sweep(); });
-        else
-            sweep();
+        {
+            // Counted work: the sweep's two passes over X (the first
+            // contraction of each half of the dimension tree).
+            SummaryScope sc(ctx, "HOOI sweep (FP64)", x_pass_flop(), x_pass_bytes());
+            if (graph && !opts.profile)
+                graph->run(ctx, [&] { sweep(); });
+            else
+                sweep();
+        }
         const double g2 = read_scalar(1);
         res = std::sqrt(std::max(0.0, 1.0 - g2 / x2));
         if (rep && it < DT_MAX_HIST) rep->res_hist[it] = res;
@@ -388,6 +412,7 @@ int dt_hooi_dense(dt_ctx *ctx, const void *X, int dtype, int ndim, const int64_t
         if (report) std::memset(report, 0, sizeof(*report));
         const size_t esz = dtype == DT_F64 ? 8 : 4;
         DevView x(ctx, X, prod(shape, ndim) * esz, true, false);
+        SummaryScope sc(ctx, "Algorithm::Tucker::HOOI_ALS()");
         if (o.precision == DT_PREC_FP64) {
             // A staged host X lives only for this call: its plan is not kept
             // and its sweeps are launched directly.

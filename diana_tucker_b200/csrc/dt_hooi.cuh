@@ -43,6 +43,8 @@ struct DenseHooi {
     void leaf(int n, const double *Y, const int64_t *shape);
     void sweep();
     double read_scalar(int k);
+    double x_pass_flop() const;
+    double x_pass_bytes() const;
 };
 
 // BF16 / split-BF16 tensor-core HOOI (dt_hooi_tc.cu).

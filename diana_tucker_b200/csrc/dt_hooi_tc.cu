@@ -208,6 +208,13 @@ struct MixedHooi {
         node(0, N, Xh.as<__nv_bfloat16>(), split ? Xl.as<__nv_bfloat16>() : nullptr, I);
     }
 
+    // 2 |X| R per X pass: each half of the tree first contracts its highest
+    // mode.
+    double x_pass_flop() const {
+        const int mid = (N + 1) / 2;
+        return 2.0 * xsize * (R[N - 1] + R[mid - 1]);
+    }
+
     double read_scalar(int k) {
         double h = 0.0;
         DT_CUDA(cudaMemcpyAsync(&h, scal.as<double>() + k, sizeof(double), cudaMemcpyDeviceToHost,
@@ -267,11 +274,17 @@ struct MixedHooi {
                 split = true;
                 prev = -1.0;
             }
-            SweepGraph *gr = split ? g_split : g_bf16;
-            if (gr && !opts.profile)
-                gr->run(ctx, [&] { sweep(); });
-            else
-                sweep();
+            {
+                // Counted work: the sweep's two passes over X (3 products per
+                // element and rank with split operands).
+                SummaryScope sc(ctx, split ? "HOOI sweep (BF16 split)" : "HOOI sweep (BF16)",
+                                x_pass_flop() * (split ? 3 : 1), 2.0 * xsize * (split ? 4 : 2));
+                SweepGraph *gr = split ? g_split : g_bf16;
+                if (gr && !opts.profile)
+                    gr->run(ctx, [&] { sweep(); });
+                else
+                    sweep();
+            }
             const double g2 = read_scalar(1);
             res = std::sqrt(std::max(0.0, 1.0 - g2 / x2));
             if (rep && it < DT_MAX_HIST) rep->res_hist[it] = res;
@@ -304,6 +317,8 @@ struct MixedHooi {
         // X x_1 U_1^T ... x_N U_N^T to FP64 rounding).
         DevMem cur;
         {
+            SummaryScope sc(ctx, "core projection (FP64)", 2.0 * xsize * R[N - 1],
+                            4.0 * xsize);
             int64_t shape[16];
             std::memcpy(shape, I, N * sizeof(int64_t));
             std::vector<int> ord(N);

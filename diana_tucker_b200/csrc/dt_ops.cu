@@ -46,6 +46,7 @@ int dt_ttm_f64(dt_ctx *ctx, const double *X, int ndim, const int64_t *shape, int
         DevView x(ctx, X, nx * sizeof(double), true, false);
         DevView m(ctx, M, J * v.I * sizeof(double), true, false);
         DevView y(ctx, Y, ny * sizeof(double), false, true);
+        SummaryScope sc(ctx, "Function::ttm()", 2.0 * nx * J, 8.0 * (nx + ny + J * v.I));
         ttm_f64<double>(ctx, x.as<double>(), v.L, v.I, v.B, m.as<double>(), 1, J, J,
                         y.as<double>());
         y.finish();
@@ -62,6 +63,8 @@ int dt_gram_f64(dt_ctx *ctx, const double *X, int ndim, const int64_t *shape, in
         const ModeView v = around(ndim, shape, mode);
         DevView x(ctx, X, v.L * v.I * v.B * sizeof(double), true, false);
         DevView g(ctx, G, v.I * v.I * sizeof(double), false, true);
+        SummaryScope sc(ctx, "Function::gram()", 2.0 * v.L * v.I * v.B * v.I,
+                        8.0 * (v.L * v.I * v.B + v.I * v.I));
         ttt_f64(ctx, x.as<double>(), x.as<double>(), v.L, v.I, v.I, v.B, g.as<double>());
         g.finish();
     });
@@ -85,6 +88,8 @@ int dt_ttt_except_f64(dt_ctx *ctx, const double *A, const int64_t *shapeA, const
         DevView a(ctx, A, va.L * va.I * va.B * sizeof(double), true, false);
         DevView b(ctx, B, va.L * IB * va.B * sizeof(double), true, false);
         DevView c(ctx, C, va.I * IB * sizeof(double), false, true);
+        SummaryScope sc(ctx, "Function::ttt_except()", 2.0 * va.L * va.I * IB * va.B,
+                        8.0 * (va.L * (va.I + IB) * va.B + va.I * IB));
         ttt_f64(ctx, a.as<double>(), b.as<double>(), va.L, va.I, IB, va.B, c.as<double>());
         c.finish();
     });
@@ -191,6 +196,9 @@ int dt_als_f64(dt_ctx *ctx, const double *Y, int ndim, const int64_t *shape, int
         DevMem work(ctx, (3 * v.I * R + R) * sizeof(double));
         DevMem flag(ctx, sizeof(int));
         DT_CUDA(cudaMemsetAsync(flag.get(), 0, sizeof(int), ctx->stream));
+        SummaryScope sc(ctx, "Algorithm::Tucker::ALS_()",
+                        2.0 * v.L * v.I * v.B * v.I + 2.0 * iters * v.I * v.I * R,
+                        8.0 * (v.L * v.I * v.B + v.I * v.I));
         ttt_f64(ctx, y.as<double>(), y.as<double>(), v.L, v.I, v.I, v.B, S.as<double>());
         DT_CUDA(cudaMemcpyAsync(q.ptr(), l0.ptr(), v.I * R * sizeof(double),
                                 cudaMemcpyDeviceToDevice, ctx->stream));

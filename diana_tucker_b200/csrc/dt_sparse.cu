@@ -1176,6 +1176,10 @@ void sp_ttmc_compact(dt_ctx *ctx, const dt_sptensor *sp, const double *const *Ut
         for (int m = 0; m < 3; m++)
             if (m != mode && m != F) E = m;
         DevMem tpart(ctx, std::max<int64_t>(mc.tslots, 1) * P * sizeof(double));
+        SummaryScope sc(ctx, "Function::ttmc()",
+                        2.0 * ((double)sp->nnz * R[E] + (double)mc.nfib * R[F] * R[E]),
+                        (double)sp->nnz * 12.0 + (double)mc.nfib * 8.0 +
+                            (double)mc.nrows * P * 8.0);
         if (timer) timer->begin();
         if (F < E)
             fib_dispatch<true>(ctx, mc, Ut_dev[F], (int)R[F], Ut_dev[E], (int)R[E], Yc,
@@ -1239,6 +1243,8 @@ void sp_ttmc_compact(dt_ctx *ctx, const dt_sptensor *sp, const double *const *Ut
 void sp_mtr(dt_ctx *ctx, const dt_sptensor *sp, const double *Yc, int mode, int P,
             const double *Un, int Rn, double *L) {
     const ModeCopy &mc = sp->modes[mode];
+    SummaryScope sc(ctx, "Function::ttmc_mTR()", 2.0 * mc.nrows * P * Rn,
+                    8.0 * mc.nrows * (P + Rn));
     DT_CHECK_ARG(Rn <= 32, "sparse ttmc_mTR: R_n (%d) must be <= 32", Rn);
     const int64_t target = 2LL * ctx->num_sms;
     const int64_t rpb = std::max<int64_t>(64, (mc.nrows + target - 1) / target);
@@ -1261,6 +1267,8 @@ void sp_mtr(dt_ctx *ctx, const dt_sptensor *sp, const double *Yc, int mode, int 
 void sp_mtl(dt_ctx *ctx, const dt_sptensor *sp, const double *Yc, int mode, int P,
             const double *L, int Rn, double *out) {
     const ModeCopy &mc = sp->modes[mode];
+    SummaryScope sc(ctx, "Function::ttmc_mTL()", 2.0 * mc.nrows * P * Rn,
+                    8.0 * mc.nrows * (P + Rn));
     DT_CHECK_ARG(Rn <= 32, "sparse ttmc_mTL: R_n (%d) must be <= 32", Rn);
     DT_CUDA(cudaMemsetAsync(out, 0, sp->shape[mode] * Rn * sizeof(double), ctx->stream));
     const int ntl = (Rn + 7) / 8;
@@ -1494,6 +1502,7 @@ int dt_sp_hooi(dt_ctx *ctx, const dt_sptensor *sp, const int64_t *R, int max_swe
         DevMem Yc(ctx, maxYc * sizeof(double));
         DevMem L(ctx, 1024 * 32 * sizeof(double));
         LaunchTimer timer(ctx, true);  // TTMc launches, reported as ttm_x_*
+        SummaryScope sc(ctx, "Algorithm::SpTucker::Sp_HOOI_ALS()");
         DT_CUDA(cudaEventRecord(ctx->ev_start, ctx->stream));
         for (int it = 0; it < max_sweeps; it++) {
             for (int n = 0; n < nd; n++) {
@@ -1502,6 +1511,8 @@ int dt_sp_hooi(dt_ctx *ctx, const dt_sptensor *sp, const int64_t *R, int max_swe
                 sp_mtr(ctx, sp, Yc.as<double>(), n, P, ptrs[n], (int)R[n], L.as<double>());
                 sp_mtl(ctx, sp, Yc.as<double>(), n, P, L.as<double>(), (int)R[n],
                        const_cast<double *>(ptrs[n]));
+                SummaryScope so(ctx, "Operator::orth2()", 2.0 * R[n] * R[n] * sp->shape[n],
+                                8.0 * R[n] * sp->shape[n]);
                 orth2_rows(ctx, const_cast<double *>(ptrs[n]), R[n], sp->shape[n]);
             }
         }

@@ -295,6 +295,46 @@ DT_API int dt_sp_ttmc_rows(dt_ctx *ctx, const dt_sptensor *sp, const double *con
 DT_API int dt_sp_hooi(dt_ctx *ctx, const dt_sptensor *sp, const int64_t *R, int max_sweeps,
                double *const *Ut, double *G, dt_hooi_report *report);
 
+/* ---- Summary profiler ---------------------------------------------------- */
+/* The reference's Summary (include/summary.hpp:27-60, src/summary.cpp):
+ * enabling starts "{Main}" (Summary::init); library operations then record
+ * named, nested ranges as CUDA events on the context's stream, each with its
+ * flop and byte counts, which also count towards the enclosing range
+ * (Summary::start / Summary::end).  Off by default. */
+DT_API int dt_summary_enable(dt_ctx *ctx, int on);
+/* Drops the recorded ranges. */
+DT_API int dt_summary_reset(dt_ctx *ctx);
+/* Closes the open ranges and writes the table of Summary::print_summary
+ * (src/summary.cpp:100-206: per name Time(s), Time C.(%), Number,
+ * Avg. Time(s), GFlop/s, Bandw.(GB/s)) into buf, NUL-terminated and cut to
+ * size bytes; *needed is the full length + 1.  Recording then restarts. */
+DT_API int dt_summary_table(dt_ctx *ctx, char *buf, int64_t size, int64_t *needed);
+
+/* ---- .tns ingest -------------------------------------------------------- */
+typedef struct dt_tns dt_tns;
+
+/* Reads a .tns text file ("i_1 ... i_N value" per line, 1-based indices,
+ * separated by spaces or tabs) and parses it on the device: a newline scan,
+ * one thread per line, dims = max index + 1 per mode, blank lines skipped.
+ * Replaces read_data<double> (src/read_data.cpp:36-129) at world size 1, which
+ * parses on one host thread.  The reference's read_double takes digits and
+ * '.' only (read_data.cpp:24-33); values here may also carry a sign and an
+ * exponent.  A line with another token count, an index below 1 or a token
+ * that is not a number fails with DT_ERR_ARG naming the line. */
+DT_API int dt_tns_read(dt_ctx *ctx, const char *path, dt_tns **out, int *ndim, int64_t *nnz);
+/* The same on a .tns image already in memory (host or device bytes). */
+DT_API int dt_tns_parse(dt_ctx *ctx, const char *bytes, int64_t size, dt_tns **out, int *ndim,
+                        int64_t *nnz);
+/* dims[ndim]; idx[m] (nnz 0-based int64 each) and vals (nnz FP64), host or
+ * device, in file order.  Any argument may be NULL to skip it.  The
+ * data_buffer<double> fields (include/read_data.hpp:9-17). */
+DT_API int dt_tns_copy(dt_ctx *ctx, const dt_tns *t, int64_t *dims, int64_t *const *idx,
+                       double *vals);
+/* The sparse tensor of the parsed nonzeros, built from the device copy
+ * (SpTensor<Ty>::SpTensor(data_buffer<Ty>*), sp_tensor.hpp:71-240). */
+DT_API int dt_tns_to_sptensor(dt_ctx *ctx, const dt_tns *t, dt_sptensor **sp);
+DT_API int dt_tns_destroy(dt_tns *t);
+
 #ifdef __cplusplus
 }
 #endif

@@ -150,3 +150,16 @@ def hooi_harness(X, ranks, max_iter, tol, U_init=None):
                                     ctypes.c_int64(max_iter), ctypes.c_double(tol),
                                     1 if U_init is None else 0, init_ptr, _d(G), Uptr, _d(hist))
     return G, U, list(hist[:sweeps])
+
+
+def read_tns(path):
+    """read_data<double> (src/read_data.cpp:36-129): (idx list of 0-based int64
+    arrays, vals, dims)."""
+    L = lib()
+    nd, nz = ctypes.c_int64(), ctypes.c_int64()
+    L.ref_read_tns(path.encode(), ctypes.byref(nd), ctypes.byref(nz))
+    dims = np.zeros(nd.value, dtype=np.int64)
+    idx = np.zeros(nd.value * nz.value, dtype=np.int64)
+    vals = np.zeros(nz.value)
+    L.ref_read_tns_copy(dims.ctypes.data_as(_i64p), idx.ctypes.data_as(_i64p), _d(vals))
+    return [idx[m * nz.value:(m + 1) * nz.value] for m in range(nd.value)], vals, dims

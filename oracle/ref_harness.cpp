@@ -229,4 +229,31 @@ int ref_hooi_harness(const double *X, int ndim, const int64_t *shape, const int6
     return sweeps;
 }
 
+// read_data<double> (src/read_data.cpp:36-129) on a .tns file: first call
+// parses and returns ndim / nnz; the second copies dims, the 0-based indices
+// (ndim x nnz, mode-major) and the values, then frees the buffers.
+static data_buffer<double> g_tns;
+
+int ref_read_tns(const char *path, int64_t *ndim, int64_t *nnz) {
+    read_data<double>(const_cast<char *>(path), &g_tns);
+    *ndim = (int64_t)g_tns.ndim;
+    *nnz = (int64_t)g_tns.nnz;
+    return 0;
+}
+
+int ref_read_tns_copy(int64_t *dims, int64_t *idx, double *vals) {
+    const size_t nd = g_tns.ndim, nz = g_tns.nnz;
+    for (size_t m = 0; m < nd; m++) {
+        dims[m] = (int64_t)g_tns.dims[m];
+        for (size_t e = 0; e < nz; e++) idx[m * nz + e] = (int64_t)g_tns.index_lists[m][e];
+        free(g_tns.index_lists[m]);
+    }
+    for (size_t e = 0; e < nz; e++) vals[e] = g_tns.vals[e];
+    free(g_tns.index_lists);
+    free(g_tns.vals);
+    free(g_tns.dims);
+    g_tns = data_buffer<double>();
+    return 0;
+}
+
 }  // extern "C"

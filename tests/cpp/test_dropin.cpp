@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <fstream>
+#include <string>
 #include <vector>
 
 #include "diana/algorithm.hpp"
@@ -114,6 +115,25 @@ int main(int argc, char **argv) {
         const double gn = G.fnorm(), an = Function::fnorm(A);
         EXPECT(gn > 0 && gn <= an * (1 + 1e-12), "sparse ||G|| %.6g vs ||A|| %.6g", gn, an);
         EXPECT(Ut.size() == 3 && Ut[0].shape()[0] == 4 && Ut[0].shape()[1] == 40, "Ut shapes");
+    }
+    // read_data on a small .tns file (1-based indices), then SpTensor from it.
+    {
+        const std::string tns = std::string(argv[1]) + ".tns";
+        const char *path = tns.c_str();
+        FILE *f = std::fopen(path, "w");
+        std::fprintf(f, "1 2 3 1.5\n4 1 2 2.25\n2 2 1 -0.5\n");
+        std::fclose(f);
+        auto *dbf = new data_buffer<double>();
+        read_data<double>(const_cast<char *>(path), dbf);
+        EXPECT(dbf->ndim == 3 && dbf->nnz == 3, "read_data ndim %zu nnz %zu", dbf->ndim, dbf->nnz);
+        EXPECT(dbf->dims[0] == 4 && dbf->dims[1] == 2 && dbf->dims[2] == 3, "read_data dims");
+        EXPECT(dbf->index_lists[0][1] == 3 && dbf->index_lists[2][0] == 2 && dbf->vals[1] == 2.25 &&
+                   dbf->vals[2] == -0.5,
+               "read_data entries");
+        SpTensor<double> A(dbf);
+        const double an = Function::fnorm(A);
+        EXPECT(std::fabs(an - std::sqrt(1.5 * 1.5 + 2.25 * 2.25 + 0.25)) < 1e-14, "fnorm %.17g", an);
+        std::remove(path);
     }
     if (failures == 0) std::printf("ALL PASSED\n");
     return failures == 0 ? 0 : 1;
