@@ -33,7 +33,7 @@ constexpr int MAXD = 8;
 constexpr int64_t CHUNK = 512;
 constexpr int FIB_CHUNK = 8;
 constexpr int64_t TASK_PACK_GRP = 64;
-constexpr int64_t TASK_PIECE_GRP = 256;
+constexpr int64_t TASK_PIECE_BATCHES = 32;
 
 struct ModeCopy {
     int64_t nrows = 0;  // non-empty rows
@@ -73,7 +73,12 @@ struct ModeCopy {
     DevMem tasks;
     int64_t tslots = 0;
     int64_t tmulti = 0;   // rows cut into several pieces
+    // Their partial rows are summed in two levels: segments of at most
+    // COMB_SEG consecutive pieces (tseg_first / tseg_count: piece slots), then
+    // each row's segments (tmulti_first / tmulti_count: segment indices).
     DevMem tmulti_row, tmulti_first, tmulti_count;
+    int64_t nseg = 0;
+    DevMem tseg_first, tseg_count;
 };
 
 struct FactorSet {
@@ -549,6 +554,26 @@ __global__ void __launch_bounds__(256) ttmc3f_wide_kernel(
 // the 4 x 4 accumulators are then added in a fixed order (deterministic).
 // ---------------------------------------------------------------------------
 constexpr int COMB_SPLIT = 4;
+constexpr int COMB_SEG = 16;
+
+// First level of the fibre path's combine: seg_out[g] = the sum, in order, of
+// the tseg_count[g] partial rows from slot tseg_first[g] (at most COMB_SEG;
+// four accumulators, fixed order).
+__global__ void __launch_bounds__(256) sum_segments_kernel(
+    const double *__restrict__ Ypart, const int32_t *__restrict__ seg_first,
+    const int32_t *__restrict__ seg_count, int64_t nseg, int P, double *__restrict__ seg_out) {
+    for (int64_t g = blockIdx.x; g < nseg; g += gridDim.x) {
+        const int64_t f = seg_first[g];
+        const int cnt = seg_count[g];
+        for (int p = threadIdx.x; p < P; p += blockDim.x) {
+            double a[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+            for (int j = 0; j < COMB_SEG; j++)
+                if (j < cnt) a[j & 3] += Ypart[(f + j) * P + p];
+            seg_out[g * P + p] = (a[0] + a[1]) + (a[2] + a[3]);
+        }
+    }
+}
 __global__ void __launch_bounds__(1024) combine_partials_kernel(
     const double *__restrict__ Ypart, const int32_t *__restrict__ multi_row,
     const int32_t *__restrict__ multi_first, const int32_t *__restrict__ multi_count,
@@ -984,7 +1009,7 @@ void build_mode_fibre(dt_ctx *ctx, dt_sptensor *sp, int n, const std::vector<Dev
     mc.nfib = (int64_t)fib_idx.size();
 
     // Tasks over groups: packs of whole rows up to TASK_PACK_GRP groups; longer
-    // rows in pieces of TASK_PIECE_GRP groups writing partial rows.  Each task
+    // rows in pieces of TASK_PIECE_BATCHES batches writing partial rows.  Each task
     // is cut into batches of at most FB_GRP groups and FB_NZ nonzeros (a group
     // holds at most 4 FIB_CHUNK <= FB_NZ).  Cost estimate for the
     // largest-first order: nonzeros + 16 per group.
@@ -995,13 +1020,14 @@ void build_mode_fibre(dt_ctx *ctx, dt_sptensor *sp, int n, const std::vector<Dev
         int64_t cost;
     };
     std::vector<Task> tasks;
-    std::vector<int32_t> tmrow, tmfirst, tmcount;
+    std::vector<int32_t> tmrow, tmfirst, tmcount, tsfirst, tscount;
     int64_t tslots = 0;
-    auto add_task = [&](int32_t q0, int32_t q1, int32_t slot) {
-        const int32_t b0 = (int32_t)bt.size();
-        int32_t q = q0;
+    // Batches of the groups [q0, q1), appended to bt; returns how many.
+    auto make_batches = [&](int32_t q0, int32_t q1) {
+        int32_t nb = 0, q = q0;
         while (q < q1) {
             bt.push_back(make_int2(q, fib_ptr[4 * q]));
+            nb++;
             int32_t nz = 0, cnt = 0;
             while (q < q1 && cnt < FB_GRP && nz + gnz(q) <= FB_NZ) {
                 nz += gnz(q);
@@ -1009,37 +1035,51 @@ void build_mode_fibre(dt_ctx *ctx, dt_sptensor *sp, int n, const std::vector<Dev
                 q++;
             }
         }
-        const int64_t cost = (int64_t)(fib_ptr[4 * q1] - fib_ptr[4 * q0]) + 16 * (int64_t)(q1 - q0);
-        tasks.push_back({make_int4(b0, (int32_t)bt.size(), slot, 0), cost});
+        return nb;
+    };
+    // A warp spends about the same time on every batch, so a task's cost is
+    // its batch count.
+    auto add_pack = [&](int32_t q0, int32_t q1) {
+        const int32_t b0 = (int32_t)bt.size();
+        const int32_t nb = make_batches(q0, q1);
+        tasks.push_back({make_int4(b0, b0 + nb, -1, 0), nb});
     };
     {
         int32_t pack_beg = -1;
         for (int64_t k = 0; k < mc.nrows; k++) {
             const int32_t b = row_grp[k], c = row_grp[k + 1] - b;
             if (c > TASK_PACK_GRP) {
-                if (pack_beg >= 0) add_task(pack_beg, b, -1);
+                if (pack_beg >= 0) add_pack(pack_beg, b);
                 pack_beg = -1;
-                const int32_t np = (int32_t)((c + TASK_PIECE_GRP - 1) / TASK_PIECE_GRP);
+                // A long row: its batches in pieces of at most TASK_PIECE_BATCHES.
+                const int32_t b0 = (int32_t)bt.size();
+                const int32_t nb = make_batches(b, b + c);
+                const int32_t np = (nb + (int32_t)TASK_PIECE_BATCHES - 1) / (int32_t)TASK_PIECE_BATCHES;
                 if (np > 1) {
                     tmrow.push_back((int32_t)k);
-                    tmfirst.push_back((int32_t)tslots);
-                    tmcount.push_back(np);
+                    tmfirst.push_back((int32_t)tsfirst.size());
+                    for (int32_t q = 0; q < np; q += COMB_SEG) {
+                        tsfirst.push_back((int32_t)tslots + q);
+                        tscount.push_back(std::min<int32_t>(COMB_SEG, np - q));
+                    }
+                    tmcount.push_back((int32_t)tsfirst.size() - tmfirst.back());
                 }
                 for (int32_t j = 0; j < np; j++) {
-                    const int32_t q0 = b + j * (int32_t)TASK_PIECE_GRP;
-                    const int32_t q1 = std::min(b + c, q0 + (int32_t)TASK_PIECE_GRP);
-                    add_task(q0, q1, np > 1 ? (int32_t)(tslots + j) : -1);
+                    const int32_t x0 = b0 + j * (int32_t)TASK_PIECE_BATCHES;
+                    const int32_t x1 = std::min(b0 + nb, x0 + (int32_t)TASK_PIECE_BATCHES);
+                    tasks.push_back({make_int4(x0, x1, np > 1 ? (int32_t)(tslots + j) : -1, 0),
+                                     x1 - x0});
                 }
                 if (np > 1) tslots += np;
                 continue;
             }
             if (pack_beg >= 0 && b + c - pack_beg > TASK_PACK_GRP) {
-                add_task(pack_beg, b, -1);
+                add_pack(pack_beg, b);
                 pack_beg = -1;
             }
             if (pack_beg < 0) pack_beg = b;
         }
-        if (pack_beg >= 0) add_task(pack_beg, ngroups, -1);
+        if (pack_beg >= 0) add_pack(pack_beg, ngroups);
         bt.push_back(make_int2(ngroups, fib_ptr[4 * ngroups]));
         std::stable_sort(tasks.begin(), tasks.end(),
                          [](const Task &a, const Task &b) { return a.cost > b.cost; });
@@ -1050,6 +1090,7 @@ void build_mode_fibre(dt_ctx *ctx, dt_sptensor *sp, int n, const std::vector<Dev
     mc.nbatch = (int64_t)bt.size() - 1;
     mc.tslots = tslots;
     mc.tmulti = (int64_t)tmrow.size();
+    mc.nseg = (int64_t)tsfirst.size();
 
     DevMem perm;
     upload(ctx, perm, order);
@@ -1069,6 +1110,8 @@ void build_mode_fibre(dt_ctx *ctx, dt_sptensor *sp, int n, const std::vector<Dev
     upload(ctx, mc.tmulti_row, tmrow);
     upload(ctx, mc.tmulti_first, tmfirst);
     upload(ctx, mc.tmulti_count, tmcount);
+    upload(ctx, mc.tseg_first, tsfirst);
+    upload(ctx, mc.tseg_count, tscount);
     DT_CUDA(cudaStreamSynchronize(ctx->stream));
 }
 
@@ -1188,9 +1231,14 @@ void sp_ttmc_compact(dt_ctx *ctx, const dt_sptensor *sp, const double *const *Ut
             fib_dispatch<false>(ctx, mc, Ut_dev[F], (int)R[F], Ut_dev[E], (int)R[E], Yc,
                                 tpart.as<double>());
         if (mc.tmulti > 0) {
+            DevMem segs(ctx, (size_t)mc.nseg * P * sizeof(double));
+            DT_LAUNCH(ctx, sum_segments_kernel,
+                      (unsigned)std::min<int64_t>(mc.nseg, 65535), 256, 0, tpart.as<double>(),
+                      mc.tseg_first.as<int32_t>(), mc.tseg_count.as<int32_t>(), mc.nseg, P,
+                      segs.as<double>());
             const unsigned blocks = (unsigned)std::min<int64_t>(mc.tmulti, 65535);
             DT_LAUNCH(ctx, combine_partials_kernel, blocks, 256 * COMB_SPLIT, 0,
-                      tpart.as<double>(), mc.tmulti_row.as<int32_t>(),
+                      segs.as<double>(), mc.tmulti_row.as<int32_t>(),
                       mc.tmulti_first.as<int32_t>(), mc.tmulti_count.as<int32_t>(), mc.tmulti, P,
                       Yc);
         }
