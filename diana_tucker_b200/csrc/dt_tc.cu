@@ -452,41 +452,59 @@ __global__ void split_f32_kernel(const float *__restrict__ x, int64_t n,
 }
 
 // Sweep core from the K-major leaf rows: G[k + K*r] = sum_i Y[i][k] U[i][r]
-// in FP64 (hi + lo converts exactly), one thread per (k, r); per-block partial
-// sum of G^2 in FP64.
+// in FP64 (hi + lo converts exactly).  A CTA owns 64 columns k; thread
+// (c, q) = (t % 64, t / 64) sums the rows i = q, q + 4, ... for all R outputs of
+// column k in registers (U staged in shared memory, row-major), and the four
+// partial sums are added in a fixed order.  Per-block partial sum of G^2.
+template <int RMAX>
 __global__ void __launch_bounds__(256) core_rows_kernel(const __nv_bfloat16 *__restrict__ Yh,
                                                         const __nv_bfloat16 *__restrict__ Yl,
                                                         int64_t I, int64_t K,
                                                         const double *__restrict__ U, int R,
                                                         double *__restrict__ G,
                                                         double *__restrict__ part) {
-    extern __shared__ double Us[];  // I x R
-    for (int64_t e = threadIdx.x; e < I * R; e += blockDim.x) Us[e] = U[e];
+    extern __shared__ double Us[];  // I x RMAX, row i at Us + i * RMAX
+    __shared__ double red[4][64];
+    __shared__ double s2w[8];
+    for (int64_t e = threadIdx.x; e < I * RMAX; e += blockDim.x) {
+        const int64_t i = e / RMAX;
+        const int r = (int)(e - i * RMAX);
+        Us[e] = r < R ? U[i + I * r] : 0.0;
+    }
     __syncthreads();
-    double s2 = 0.0;
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < K * R;
-         e += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t k = e % K;
-        const int r = (int)(e / K);
-        const double *u = Us + (int64_t)I * r;
-        double acc = 0.0;
-        for (int64_t i = 0; i < I; i++) {
+    const int c = threadIdx.x & 63, q = threadIdx.x >> 6;
+    const int64_t k = (int64_t)blockIdx.x * 64 + c;
+    const bool okk = k < K;
+    double acc[RMAX];
+#pragma unroll
+    for (int r = 0; r < RMAX; r++) acc[r] = 0.0;
+    if (okk) {
+        for (int64_t i = q; i < I; i += 4) {
             double y = (double)__bfloat162float(Yh[i * K + k]);
             if (Yl) y += (double)__bfloat162float(Yl[i * K + k]);
-            acc = fma(y, u[i], acc);
+            const double *u = Us + i * RMAX;
+#pragma unroll
+            for (int r = 0; r < RMAX; r++) acc[r] = fma(y, u[r], acc[r]);
         }
-        G[k + K * r] = acc;
-        s2 = fma(acc, acc, s2);
     }
-    __shared__ double red[32];
+    double s2 = 0.0;
+#pragma unroll
+    for (int r = 0; r < RMAX; r++) {
+        if (r >= R) break;
+        red[q][c] = acc[r];
+        __syncthreads();
+        if (q == 0 && okk) {
+            const double g = (red[0][c] + red[1][c]) + (red[2][c] + red[3][c]);
+            G[k + K * r] = g;
+            s2 = fma(g, g, s2);
+        }
+        __syncthreads();
+    }
+    // s2 lives in the 64 threads of q == 0 (warps 0 and 1).
     for (int o = 16; o > 0; o >>= 1) s2 += __shfl_down_sync(0xffffffffu, s2, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s2;
+    if ((threadIdx.x & 31) == 0) s2w[threadIdx.x >> 5] = s2;
     __syncthreads();
-    if (threadIdx.x < 32) {
-        s2 = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
-        for (int o = 16; o > 0; o >>= 1) s2 += __shfl_down_sync(0xffffffffu, s2, o);
-        if (threadIdx.x == 0) part[blockIdx.x] = s2;
-    }
+    if (threadIdx.x == 0) part[blockIdx.x] = s2w[0] + s2w[1];
 }
 
 __global__ void sum_double_kernel(const double *__restrict__ part, int n, double *__restrict__ out) {
@@ -677,12 +695,22 @@ void split_f32(dt_ctx *ctx, const float *x, int64_t n, __nv_bfloat16 *hi, __nv_b
 void core_rows(dt_ctx *ctx, const __nv_bfloat16 *Yh, const __nv_bfloat16 *Yl, int64_t I, int64_t K,
                const double *U, int64_t R, double *G, double *g2_out) {
     DT_CHECK_ARG(R <= 32, "core_rows: R %lld > 32", (long long)R);
-    const int blocks = std::max(1, std::min<int>(4 * ctx->num_sms, (int)ceil_div(K * R, 256)));
+    const int blocks = (int)std::max<int64_t>(1, ceil_div(K, 64));
     DevMem part(ctx, (size_t)blocks * sizeof(double));
-    const size_t smem = (size_t)I * R * sizeof(double);
-    smem_limit(ctx, core_rows_kernel, smem);
-    DT_LAUNCH(ctx, core_rows_kernel, blocks, 256, smem, Yh, Yl, I, K, U, (int)R,
-              G, part.as<double>());
+#define DT_CORE_ROWS(RM)                                                                     \
+    do {                                                                                     \
+        const size_t smem = (size_t)I * RM * sizeof(double);                                 \
+        smem_limit(ctx, core_rows_kernel<RM>, smem);                                         \
+        DT_LAUNCH(ctx, core_rows_kernel<RM>, blocks, 256, smem, Yh, Yl, I, K, U, (int)R, G,  \
+                  part.as<double>());                                                        \
+    } while (0)
+    if (R <= 8)
+        DT_CORE_ROWS(8);
+    else if (R <= 16)
+        DT_CORE_ROWS(16);
+    else
+        DT_CORE_ROWS(32);
+#undef DT_CORE_ROWS
     DT_LAUNCH(ctx, sum_double_kernel, 1, 1024, 0, part.as<double>(), blocks, g2_out);
 }
 
