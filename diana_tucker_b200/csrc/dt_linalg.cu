@@ -1183,12 +1183,30 @@ __global__ void __launch_bounds__(256) rows_apply_mma_kernel(const double *__res
     }
 }
 
-__global__ void sum_parts_kernel(const double *__restrict__ part, int nblk, int n,
-                                 double *__restrict__ out) {
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
-        double sacc = 0.0;
-        for (int b = 0; b < nblk; b++) sacc += part[(int64_t)b * n + e];
-        out[e] = sacc;
+// out[e] = sum_b part[b * n + e]: 64 outputs per CTA, 4 threads per output
+// each summing every 4th block into 4 accumulators (16 loads in flight), then
+// a fixed-order add (deterministic).
+__global__ void __launch_bounds__(256) sum_parts_kernel(const double *__restrict__ part, int nblk,
+                                                        int n, double *__restrict__ out) {
+    __shared__ double red[4][64];
+    const int s = threadIdx.x >> 6, o = threadIdx.x & 63;
+    for (int e0 = blockIdx.x * 64; e0 < n; e0 += gridDim.x * 64) {
+        const int e = e0 + o;
+        double a[4] = {0.0, 0.0, 0.0, 0.0};
+        if (e < n) {
+            int b = s;
+            for (; b + 12 < nblk; b += 16) {
+#pragma unroll
+                for (int j = 0; j < 4; j++) a[j] += part[(int64_t)(b + 4 * j) * n + e];
+            }
+#pragma unroll
+            for (int j = 0; j < 3; j++)
+                if (b + 4 * j < nblk) a[j] += part[(int64_t)(b + 4 * j) * n + e];
+        }
+        red[s][o] = (a[0] + a[1]) + (a[2] + a[3]);
+        __syncthreads();
+        if (s == 0 && e < n) out[e] = (red[0][o] + red[1][o]) + (red[2][o] + red[3][o]);
+        __syncthreads();
     }
 }
 
@@ -1361,7 +1379,8 @@ void orth2_rows(dt_ctx *ctx, double *A, int64_t len1, int64_t len2) {
     do {                                                                                        \
         DT_LAUNCH(ctx, rows_gram_mma_kernel<R>, nblk, 256, 0, src, r, len2, rpb,                \
                   part.as<double>());                                                           \
-        DT_LAUNCH(ctx, sum_parts_kernel, 1, 256, 0, part.as<double>(), nblk, r * r,             \
+        DT_LAUNCH(ctx, sum_parts_kernel, ceil_div(r * r, 64), 256, 0, part.as<double>(), nblk,    \
+                  r * r,                                                                     \
                   G.as<double>());                                                              \
         DT_LAUNCH(ctx, chol_lower_inv_kernel, 1, 256, 2 * r * r * sizeof(double), G.as<double>(), \
                   r, Li.as<double>(), flag.as<int>());                                          \

@@ -645,16 +645,26 @@ __global__ void __launch_bounds__(256) mtl_mma_kernel(const double *__restrict__
         double acc[NTL][2];
 #pragma unroll
         for (int j = 0; j < NTL; j++) acc[j][0] = acc[j][1] = 0.0;
-#pragma unroll 8
-        for (int kk = 0; kk < ksteps; kk++) {
-            const int p = 4 * kk + t;
-            const double a = (okr && p < P) ? y[p] : 0.0;
+        // Eight k-steps of Y loads are issued before their MMAs.
+        for (int k0 = 0; k0 < ksteps; k0 += 8) {
+            double av[8];
 #pragma unroll
-            for (int j = 0; j < NTL; j++) {
-                const int r = 8 * j + g;
-                const double b = LSM ? Ls[p * LDL + r]
-                                     : ((p < P && r < Rn) ? __ldg(L + p + (int64_t)P * r) : 0.0);
-                sp_dmma(acc[j][0], acc[j][1], a, b);
+            for (int u = 0; u < 8; u++) {
+                const int p = 4 * (k0 + u) + t;
+                av[u] = (okr && k0 + u < ksteps && p < P) ? y[p] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                if (k0 + u >= ksteps) break;
+                const int p = 4 * (k0 + u) + t;
+#pragma unroll
+                for (int j = 0; j < NTL; j++) {
+                    const int r = 8 * j + g;
+                    const double b =
+                        LSM ? Ls[p * LDL + r]
+                            : ((p < P && r < Rn) ? __ldg(L + p + (int64_t)P * r) : 0.0);
+                    sp_dmma(acc[j][0], acc[j][1], av[u], b);
+                }
             }
         }
         if (okr) {
