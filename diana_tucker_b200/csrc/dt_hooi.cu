@@ -256,6 +256,12 @@ double DenseHooi::x_pass_bytes() const {
     return 2.0 * xsize * (dtype == DT_F64 ? 8 : 4);
 }
 
+void DenseHooi::read_scalars(int k, int n, double *out) {
+    DT_CUDA(cudaMemcpyAsync(out, scal.as<double>() + k, n * sizeof(double),
+                            cudaMemcpyDeviceToHost, ctx->stream));
+    DT_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
 double DenseHooi::read_scalar(int k) {
     double h = 0.0;
     DT_CUDA(cudaMemcpyAsync(&h, scal.as<double>() + k, sizeof(double), cudaMemcpyDeviceToHost,
@@ -272,7 +278,8 @@ void DenseHooi::run(double *G_user, double *const *U_user, dt_hooi_report *rep,
     DT_CUDA(cudaEventRecord(ctx->ev_start, ctx->stream));
     sumsq(ctx, Xdev, dtype, xsize, scal.as<double>());
     init_factors(U_user);
-    const double x2 = read_scalar(0);
+    // ||X||^2 is read with the first sweep's ||G||^2 (one synchronisation).
+    double x2 = -1.0;
     double prev = -1.0, res = 0.0;
     int sweeps = 0;
     for (int it = 0; it < opts.max_sweeps; it++) {
@@ -285,7 +292,15 @@ void DenseHooi::run(double *G_user, double *const *U_user, dt_hooi_report *rep,
             else
                 sweep();
         }
-        const double g2 = read_scalar(1);
+        double g2;
+        if (x2 < 0.0) {
+            double xg[2];
+            read_scalars(0, 2, xg);
+            x2 = xg[0];
+            g2 = xg[1];
+        } else {
+            g2 = read_scalar(1);
+        }
         res = std::sqrt(std::max(0.0, 1.0 - g2 / x2));
         if (rep && it < DT_MAX_HIST) rep->res_hist[it] = res;
         sweeps = it + 1;
@@ -295,6 +310,7 @@ void DenseHooi::run(double *G_user, double *const *U_user, dt_hooi_report *rep,
         if (opts.tol > 0 && prev >= 0 && std::fabs(res - prev) < opts.tol) break;
         prev = res;
     }
+    if (x2 < 0.0) x2 = read_scalar(0);
     if (sweeps == 0) {
         // No sweep requested: the core of the initial factors.
         int64_t shape[16];

@@ -43,6 +43,7 @@ struct DenseHooi {
     void leaf(int n, const double *Y, const int64_t *shape);
     void sweep();
     double read_scalar(int k);
+    void read_scalars(int k, int n, double *out);
     double x_pass_flop() const;
     double x_pass_bytes() const;
 };

@@ -215,6 +215,12 @@ struct MixedHooi {
         return 2.0 * xsize * (R[N - 1] + R[mid - 1]);
     }
 
+    void read_scalars(int k, int n, double *out) {
+        DT_CUDA(cudaMemcpyAsync(out, scal.as<double>() + k, n * sizeof(double),
+                                cudaMemcpyDeviceToHost, ctx->stream));
+        DT_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+
     double read_scalar(int k) {
         double h = 0.0;
         DT_CUDA(cudaMemcpyAsync(&h, scal.as<double>() + k, sizeof(double), cudaMemcpyDeviceToHost,
@@ -255,7 +261,8 @@ struct MixedHooi {
         for (int m = 0; m < N; m++)
             DT_CUDA(cudaMemcpyAsync(U[m].get(), helper.U[m].get(), I[m] * R[m] * sizeof(double),
                                     cudaMemcpyDeviceToDevice, ctx->stream));
-        const double x2 = read_scalar(0);
+        // ||X||^2 is read with the first sweep's ||G||^2 (one synchronisation).
+        double x2 = -1.0;
         // Phases: BF16 sweeps until the residual settles to the BF16 noise
         // floor (kBf16Settle) or kBf16Max sweeps, then split hi+lo sweeps:
         // `refine_sweeps` of them (DT_PREC_BF16), or until the residual
@@ -285,7 +292,15 @@ struct MixedHooi {
                 else
                     sweep();
             }
-            const double g2 = read_scalar(1);
+            double g2;
+            if (x2 < 0.0) {
+                double xg[2];
+                read_scalars(0, 2, xg);
+                x2 = xg[0];
+                g2 = xg[1];
+            } else {
+                g2 = read_scalar(1);
+            }
             res = std::sqrt(std::max(0.0, 1.0 - g2 / x2));
             if (rep && it < DT_MAX_HIST) rep->res_hist[it] = res;
             sweeps = it + 1;
@@ -313,6 +328,7 @@ struct MixedHooi {
                 }
             }
         }
+        if (x2 < 0.0) x2 = read_scalar(0);
         // Final core, FP64 projection from the original X (the returned G is
         // X x_1 U_1^T ... x_N U_N^T to FP64 rounding).
         DevMem cur;

@@ -45,6 +45,21 @@ def test_ttmc_rows_mtr_mtl(ctx, oracle_sparse, zipf_small, R):
     sp.close()
 
 
+@pytest.mark.parametrize("R", [(4, 40, 24), (33, 2, 30)])
+def test_ttmc_wide_ranks(ctx, oracle_sparse, zipf_small, R):
+    """Other-mode ranks above 32 (P <= 1024) take the wide fibre kernel."""
+    idx, vals, shape = zipf_small
+    sp = ctx.sptensor(idx, vals, shape)
+    Ut = _factors(shape, R, 7)
+    for mode in range(3):
+        P = int(np.prod([R[m] for m in range(3) if m != mode]))
+        if P > 1024:
+            continue
+        Y = sp.ttmc_rows(Ut, R, mode)
+        assert _rel(Y, oracle_sparse.ttmc_rows(idx, vals, shape, Ut, R, mode)) < 1e-12
+    sp.close()
+
+
 def test_sparse_four_way_generic_path(ctx, oracle_sparse):
     from diana_tucker_b200 import datasets
     idx, vals, shape = datasets.sparse_zipf((60, 40, 30, 20), 5000, alpha=1.1, seed=4)
