@@ -287,6 +287,113 @@ __global__ void __launch_bounds__(TTM_NT) ttm_pipe_kernel(const TX *__restrict__
     }
 }
 
+// The ROWS layout on the FP64 tensor cores (mma.sync m8n8k4 .f64), J tile 16.
+// The CTA's 256 rows and 16 k of X (and the 16 x 16 slice of M) are staged as
+// in ttm_pipe_kernel; warp w owns rows 64 w .. 64 w + 63 as 8 x 2 tiles of 8 x 8
+// accumulators.  Per 4-k step a lane converts its 8 A elements (row g of each
+// tile, k = t) to FP64 and reads its 2 B elements; 16 mma.sync follow.  The
+// staged rows are padded by 32 bytes (X) and the M rows are 20 doubles apart,
+// so the four k-rows of a fragment load fall in different banks (64-bit loads
+// are served per half-warp).
+__device__ __forceinline__ void ttm_dmma884(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+template <class TX>
+__host__ __device__ constexpr int ttm_dm_xrow() { return TTM_BP + 32 / (int)sizeof(TX); }  // staged X row pitch
+constexpr int TTM_DM_MROW = 20;                                         // staged M row pitch
+
+template <class TX>
+__global__ void __launch_bounds__(TTM_NT) ttm_dmma_kernel(const TX *__restrict__ X, int64_t L,
+                                                          int64_t I, int64_t P,
+                                                          const double *__restrict__ M,
+                                                          int64_t msj, int64_t msi, int64_t J,
+                                                          double *__restrict__ Y, int64_t kchunk,
+                                                          int64_t ysize) {
+    constexpr int EV = 16 / sizeof(TX);
+    constexpr int TTM_DM_XROW = ttm_dm_xrow<TX>();
+    extern __shared__ __align__(16) uint8_t dm_smem[];
+    auto Ms = reinterpret_cast<double(*)[TTM_BK * TTM_DM_MROW]>(dm_smem);
+    auto Xs = reinterpret_cast<TX(*)[TTM_BK * TTM_DM_XROW]>(
+        dm_smem + 2 * TTM_BK * TTM_DM_MROW * sizeof(double));
+    const int t = threadIdx.x, w = t >> 5, lane = t & 31, g = lane >> 2, t4 = lane & 3;
+    const int64_t p0 = (int64_t)blockIdx.x * TTM_BP;
+    const int64_t j0 = (int64_t)blockIdx.y * 16;
+    const int64_t ibeg = (int64_t)blockIdx.z * kchunk;
+    const int64_t iend = min(I, ibeg + kchunk);
+    Y += (int64_t)blockIdx.z * ysize;
+    const int64_t nch = (iend - ibeg + TTM_BK - 1) / TTM_BK;
+    const int64_t b0 = p0 / L;
+    const int64_t l0 = p0 - b0 * L;
+    const TX *xb = X + l0 + L * I * b0;
+
+    auto issue = [&](int64_t c, int st) {
+        const int64_t i0 = ibeg + c * TTM_BK;
+        constexpr int PER_K = TTM_BP / EV;
+        for (int e = t; e < TTM_BK * PER_K; e += TTM_NT) {
+            const int k = e / PER_K, q = e - k * PER_K;
+            const int64_t i = i0 + k;
+            const bool ok = i < iend;
+            cp_async16(&Xs[st][k * TTM_DM_XROW + q * EV], ok ? xb + L * i + q * EV : X, ok ? 16 : 0);
+        }
+        for (int e = t; e < TTM_BK * 16; e += TTM_NT) {
+            const int k = e >> 4, j = e & 15;
+            const int64_t i = i0 + k, jj = j0 + j;
+            const bool ok = i < iend && jj < J;
+            cp_async8(&Ms[st][k * TTM_DM_MROW + j], ok ? M + jj * msj + i * msi : M, ok ? 8 : 0);
+        }
+        cp_async_commit();
+    };
+
+    double acc[8][2][2];
+#pragma unroll
+    for (int m = 0; m < 8; m++)
+#pragma unroll
+        for (int n = 0; n < 2; n++) acc[m][n][0] = acc[m][n][1] = 0.0;
+
+    if (nch > 0) issue(0, 0);
+    for (int64_t c = 0; c < nch; c++) {
+        const int st = (int)(c & 1);
+        if (c + 1 < nch) {
+            issue(c + 1, st ^ 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < TTM_BK / 4; kk++) {
+            const int k = 4 * kk + t4;
+            const double b0v = Ms[st][k * TTM_DM_MROW + g];
+            const double b1v = Ms[st][k * TTM_DM_MROW + 8 + g];
+            const TX *xr = &Xs[st][k * TTM_DM_XROW + 64 * w + g];
+#pragma unroll
+            for (int m = 0; m < 8; m++) {
+                const double a = (double)xr[8 * m];
+                ttm_dmma884(acc[m][0][0], acc[m][0][1], a, b0v);
+                ttm_dmma884(acc[m][1][0], acc[m][1][1], a, b1v);
+            }
+        }
+        __syncthreads();
+    }
+
+    // D[row g][col 2 t + h] of tile (m, n): row 64 w + 8 m + g, j = 8 n + 2 t + h.
+    double *y = Y + l0 + L * J * b0;
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+        const int64_t row = 64 * w + 8 * m + g;
+#pragma unroll
+        for (int n = 0; n < 2; n++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int64_t j = j0 + 8 * n + 2 * t4 + h;
+                if (j < J) y[row + L * j] = acc[m][n][h];
+            }
+    }
+}
+
 __global__ void sum_splits_kernel(const double *__restrict__ part, int nsplit, int64_t n,
                                   double *__restrict__ out) {
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
@@ -322,8 +429,14 @@ void ttm_launch(dt_ctx *ctx, const TX *X, int64_t L, int64_t I, int64_t B, const
     const size_t smem_rows = 2 * TTM_BK * JT * sizeof(double) + 2 * TTM_BK * TTM_BP * sizeof(TX);
     const size_t smem_kfast =
         2 * TTM_BK * JT * sizeof(double) + 2 * TTM_BP * (TTM_BK + EV) * sizeof(TX);
+    const size_t smem_dmma = 2 * TTM_BK * TTM_DM_MROW * sizeof(double) +
+                             2 * TTM_BK * ttm_dm_xrow<TX>() * sizeof(TX);
     auto launch = [&](double *dst) {
-        if (rows_ok) {
+        if (JT == 16 && rows_ok) {
+            smem_limit(ctx, ttm_dmma_kernel<TX>, smem_dmma);
+            DT_LAUNCH(ctx, ttm_dmma_kernel<TX>, grid, TTM_NT, smem_dmma, X, L, I, P, M, msj, msi,
+                      J, dst, kchunk, ysize);
+        } else if (rows_ok) {
             smem_limit(ctx, ttm_pipe_kernel<TX, JT, false>, smem_rows);
             DT_LAUNCH(ctx, (ttm_pipe_kernel<TX, JT, false>), grid, TTM_NT, smem_rows, X, L, I, P,
                       M, msj, msi, J, dst, kchunk, ysize);

@@ -42,7 +42,10 @@ def test_ops_vs_reference_fixture(ctx):
 
 @pytest.mark.parametrize("shape,J", [
     ((200, 200, 10), 10), ((37, 19, 23), 20), ((96, 96, 96), 16), ((1, 5, 7), 3),
-    ((5, 1, 7), 2), ((6, 5, 4, 3, 2), 4), ((300,), 7), ((17, 33), 33), ((4, 1000), 1)])
+    ((5, 1, 7), 2), ((6, 5, 4, 3, 2), 4), ((300,), 7), ((17, 33), 33), ((4, 1000), 1),
+    # Runs of 256 rows with 9..16 outputs: the FP64 tensor-core kernel, with
+    # and without split contraction, with a ragged J tile.
+    ((256, 40, 3), 12), ((512, 300), 16), ((16, 16, 33, 2), 9), ((256, 2, 70), 25)])
 def test_ttm_shapes(ctx, shape, J):
     rng = np.random.default_rng(hash((shape, J)) % 2**32)
     X = np.asfortranarray(rng.standard_normal(shape))
@@ -172,12 +175,13 @@ def test_hooi_200cube_hosvd_tol_vs_reference_harness(ctx, oracle_ref):
     assert abs(rep["residual"] - hist[-1]) <= 1e-10
 
 
-def test_hooi_fp32_input_equals_upcast(ctx):
+@pytest.mark.parametrize("shape,ranks", [((24, 20, 16), (4, 4, 3)),
+                                         ((16, 16, 48), (12, 12, 10))])
+def test_hooi_fp32_input_equals_upcast(ctx, shape, ranks):
     from diana_tucker_b200 import datasets
-    X32 = datasets.tucker_dense((24, 20, 16), (4, 4, 3), noise_var=1e-4, seed=9,
-                                dtype=np.float32)
-    G1, U1, r1 = ctx.hooi_dense(X32, (4, 4, 3), init="hosvd", max_sweeps=5)
-    G2, U2, r2 = ctx.hooi_dense(X32.astype(np.float64), (4, 4, 3), init="hosvd", max_sweeps=5)
+    X32 = datasets.tucker_dense(shape, ranks, noise_var=1e-4, seed=9, dtype=np.float32)
+    G1, U1, r1 = ctx.hooi_dense(X32, ranks, init="hosvd", max_sweeps=5)
+    G2, U2, r2 = ctx.hooi_dense(X32.astype(np.float64), ranks, init="hosvd", max_sweeps=5)
     assert abs(r1["g_norm"] - r2["g_norm"]) <= 1e-12 * r2["g_norm"]
     for n in range(3):
         assert dense.principal_angle_max(U1[n], U2[n]) < 1e-10
