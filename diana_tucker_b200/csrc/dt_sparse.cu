@@ -228,6 +228,8 @@ __device__ __forceinline__ void sp_dmma(double &d0, double &d1, double a, double
 constexpr int FB_NZ = 32;
 constexpr int FB_GRP = 4;
 constexpr int FB_SLOTS = 4 * FB_GRP;
+// One lane per staged nonzero and per fibre slot.
+static_assert(FB_NZ <= 32 && FB_SLOTS <= 32 && 4 * FIB_CHUNK <= FB_NZ, "batch limits");
 constexpr int FB_ROW_END = 1 << 8;  // grp_aux: the group is the last of its row
 
 // A staged factor row of up to 8 T entries has a pitch of 8 T doubles.  Four
@@ -383,7 +385,7 @@ __global__ void __launch_bounds__(256, 2) ttmc3f_kernel(
         double *vv = vv_of(buf);
         int *fo = fo_of(buf);
         int *gr = fo + FB_SLOTS + 1;
-        vv[lane] = m.v;
+        if (lane < FB_NZ) vv[lane] = m.v;
         if (lane < 4 * m.ng) fo[lane] = m.fofs;
         if (lane == 0) fo[4 * m.ng] = m.nzn;
         if (lane < m.ng) {
