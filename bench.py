@@ -93,8 +93,13 @@ class ClockSampler:
         self.nvml = None
         self.stop_ev = threading.Event()
         self.t = None
+        self.switch = sys.getswitchinterval()
 
     def start(self):
+        # The timed region is a few ms of Python issuing graph launches; a
+        # short GIL switch interval lets the polling thread run inside it.
+        self.switch = sys.getswitchinterval()
+        sys.setswitchinterval(0.0002)
         try:
             import pynvml as nv
             nv.nvmlInit()
@@ -135,6 +140,7 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def stop(self):
+        sys.setswitchinterval(self.switch)
         if self.nvml is not None:
             self.stop_ev.set()
             self.t.join(timeout=5)
