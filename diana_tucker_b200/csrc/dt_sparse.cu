@@ -32,8 +32,8 @@ namespace {
 constexpr int MAXD = 8;
 constexpr int64_t CHUNK = 512;
 constexpr int FIB_CHUNK = 8;
-constexpr int64_t TASK_PACK_GRP = 64;
-constexpr int64_t TASK_PIECE_BATCHES = 32;
+constexpr int64_t TASK_PACK_GRP = 128;
+constexpr int64_t TASK_PIECE_BATCHES = 64;
 
 struct ModeCopy {
     int64_t nrows = 0;  // non-empty rows
