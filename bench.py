@@ -70,6 +70,61 @@ def _oracle_residual():
         return None, None
 
 
+def _oracle_core_and_factors():
+    """||G|| and the factors of the reference's converged run on this tensor."""
+    try:
+        import numpy as np
+        with open(os.path.join(ROOT, "tests", "golden", "large_oracle.json")) as f:
+            g = float(json.load(f)["dense_96x4_r16"]["g_norm"])
+        z = np.load(os.path.join(ROOT, "tests", "golden", "large_oracle_factors.npz"))
+        return g, [z[f"dense_96x4_r16_U{n}"] for n in range(4)]
+    except Exception:
+        return None, None
+
+
+def _principal_angle(A, B):
+    """Largest principal angle between span(A) and span(B), from the sine
+    ||(I - Qa Qa^T) Qb||_2 (accurate for tiny angles)."""
+    import numpy as np
+    qa, _ = np.linalg.qr(np.asarray(A, dtype=np.float64))
+    qb, _ = np.linalg.qr(np.asarray(B, dtype=np.float64))
+    s = np.linalg.norm(qb - qa @ (qa.T @ qb), 2)
+    return float(np.arcsin(min(1.0, s)))
+
+
+def _config(world):
+    """The workload description shared by both arms (ours and --impl reference)."""
+    return {
+        "workload": "dense 96x96x96x96 FP32 Tucker(16^4, core*0.9^(i+j+k+l)) + N(0,1e-6), "
+                    "seed 1; HOOI ranks 16^4 to the FP64 oracle's rel-err (within 1e-6)",
+        "ours": "BF16 tcgen05 TTM chain + Gram with split hi/lo operands, FP64 subspace "
+                "iteration (2 steps per mode) / fit / final core projected from X",
+        "reference": "the reference's HOOI_ALS (compiled from its sources, FP64, all host "
+                     "threads), random init, as many sweeps as its own converged run needs",
+        "init": "libc-seeded Gaussian + QR (seed 1)",
+        "stop": "ours: split hi+lo BF16 sweeps until the residual changes by < 5e-6 (the "
+                "split-precision noise floor), then the FP64 core projection; reference: "
+                "the sweep count of its converged run (residual change < 1e-9)",
+        "target": f"|rel-err - FP64 oracle rel-err| <= {TARGET}",
+        "l2": "inputs larger than L2 (X: 340 MB FP32, 170 MB per BF16 half; L2 126 MB)",
+        "outputs": "G and U stay in HBM (CUDA tensors); e2e copies them to the host",
+        "plans": "repeated calls reuse the context's cached plan and captured sweep "
+                 "graphs (built in warm-up), for both the mixed and the FP64 path",
+        "parallelism": f"replicas x{world} (no data-path collective)",
+    }
+
+
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 class ClockSampler:
     """SM clocks and throttle reasons sampled during the timed region: NVML
     polled every ~2 ms from a thread (a timed region of a few ms still gets
@@ -264,7 +319,7 @@ def run_ours(args):
     ev0.record()
     reps = []
     for _ in range(args.steps):
-        _, _, rep = mixed()
+        _, Ulast, rep = mixed()
         reps.append(rep)
     ev1.record()
     torch.cuda.synchronize()
@@ -317,6 +372,12 @@ def run_ours(args):
     oracle_res, oracle_sweeps = _oracle_residual()
     ref_res = oracle_res if oracle_res is not None else r64["residual"]
     err = abs(rep["residual"] - ref_res)
+    # The last timed decomposition against the reference's converged run:
+    # core norm and the largest principal angle per mode.
+    oracle_g, oracle_U = _oracle_core_and_factors()
+    g_gap = abs(rep["g_norm"] - oracle_g) / oracle_g if oracle_g else None
+    angles = ([_principal_angle(Ulast[n].cpu().numpy(), oracle_U[n]) for n in range(4)]
+              if oracle_U else None)
 
     peak, peak_kind = _peaks()
     per_launch_ms = rep["ttm_x_ms"] / max(1, rep["ttm_x_launches"])
@@ -342,25 +403,13 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "bf16",
         "data": "synthetic (seeded Tucker tensor, generated in-process)",
-        "config": {
-            "workload": "dense 96x96x96x96 FP32 Tucker(16^4, core*0.9^(i+j+k+l)) + N(0,1e-6), "
-                        "seed 1; HOOI ranks 16^4; BF16 tcgen05 TTM chain + Gram with split "
-                        "hi/lo operands, FP64 subspace iteration (2 steps per mode) / fit / "
-                        "final core projected from X",
-            "init": "libc-seeded Gaussian + QR (seed 1)",
-            "stop": "split hi+lo BF16 sweeps until the residual changes by < 5e-6 "
-                    "(the split-precision noise floor); then the FP64 core projection",
-            "target": f"|rel-err - FP64 oracle rel-err| <= {TARGET}",
-            "l2": "inputs larger than L2 (X: 340 MB FP32, 170 MB per BF16 half; L2 126 MB)",
-            "outputs": "G and U stay in HBM (CUDA tensors); e2e copies them to the host",
-            "plans": "repeated calls reuse the context's cached plan and captured sweep "
-                     "graphs (built in warm-up), for both the mixed and the FP64 path",
-            "parallelism": f"replicas x{world} (no data-path collective)",
-        },
+        "config": _config(world),
         "rel_err": rep["residual"],
         "rel_err_oracle": ref_res,
         "rel_err_gap": err,
         "target_met": bool(err <= TARGET),
+        "g_norm_rel_gap": g_gap,
+        "principal_angles_vs_oracle": angles,
         "sweeps": rep["sweeps"],
         "fp64_gpu": {"ms": round(fp64_ms, 4), "rel_err": r64["residual"], "sweeps": r64["sweeps"],
                      "x_dtype": "f64",
@@ -394,7 +443,7 @@ def run_ours(args):
         _log("learned warm start")
         out["warmstart"] = _warmstart(ctx, args.ws_train, args.ws_eval)
     if rank == 0 and world == 1 and args.cpu:
-        _log("CPU baseline (reference HOOI_ALS, one sweep)")
+        _log("CPU baseline (reference HOOI_ALS)")
         out["cpu_baseline"] = _cpu_baseline(X, oracle_sweeps or r64["sweeps"])
     _log("done")
     ctx.close()
@@ -472,7 +521,8 @@ def _warmstart(ctx, n_train, n_eval):
 def _cpu_baseline(X32, sweeps):
     """The reference's HOOI_ALS (compiled from its sources with a size-1 MPI
     shim and OpenBLAS; all host threads) on the same tensor upcast to FP64:
-    one sweep timed, extrapolated to the sweeps the oracle needs."""
+    one stock call of `sweeps` sweeps (random init, the sweeps its converged
+    run needs), about 20 s of CPU work."""
     import numpy as np
     from oracle import ref
     if not ref.available():
@@ -480,17 +530,22 @@ def _cpu_baseline(X32, sweeps):
                 "sample": "unavailable: oracle/_ref/libdiana_ref.so not built"}
     X = X32.astype(np.float64)
     t0 = time.perf_counter()
-    ref.hooi_als(X, RANKS, 1, seed=1)
-    one = (time.perf_counter() - t0) * 1e3
-    return {"value": round(one * sweeps, 1), "unit": "ms", "kind": "reference",
-            "cores": os.cpu_count(),
-            "sample": f"one HOOI_ALS sweep (init + 1 sweep + core) = {one:.0f} ms, "
-                      f"x {sweeps} sweeps to converge"}
+    gn, xn = ref.hooi_als_mt(X, RANKS, sweeps, 1, 0)
+    ms = (time.perf_counter() - t0) * 1e3
+    res = float(np.sqrt(max(0.0, 1.0 - gn * gn / (xn * xn))))
+    return {"value": round(ms, 1), "unit": "ms", "kind": "reference",
+            "cores": os.cpu_count(), "cpu_model": _cpu_model(),
+            "rel_err": res,
+            "sample": f"one stock HOOI_ALS(X, 16^4, {sweeps}) call on the whole 96^4 tensor "
+                      f"(FP64, {os.cpu_count()} OpenMP threads + OpenBLAS threads)"}
 
 
 def run_reference(args):
-    """The reference's own CPU HOOI on the same workload (rank 0 only)."""
+    """The reference's own CPU HOOI on the same workload (rank 0 only): each
+    step is one stock HOOI_ALS(X, R, sweeps) call on the whole tensor with all
+    host threads, `sweeps` being its own converged run's sweep count."""
     import numpy as np
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -503,26 +558,32 @@ def run_reference(args):
                           "unavailable": "oracle/_ref/libdiana_ref.so was not built"}))
         return
     X = datasets.dense_96x4_fp32().astype(np.float64)
+    _log(f"reference: {args.warmup} warm-up + {args.steps} timed HOOI_ALS calls "
+         f"({sweeps} sweeps each)")
     for _ in range(args.warmup):
-        ref.hooi_als(X, RANKS, 1, seed=1)
-    t = []
+        ref.hooi_als_mt(X, RANKS, sweeps, 1, 0)
+    t, res = [], []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        ref.hooi_als(X, RANKS, 1, seed=1)
+        gn, xn = ref.hooi_als_mt(X, RANKS, sweeps, 1, 0)
         t.append((time.perf_counter() - t0) * 1e3)
-    one = float(np.median(t))
-    v = one * sweeps
+        res.append(float(np.sqrt(max(0.0, 1.0 - gn * gn / (xn * xn)))))
+    v = float(np.mean(t))
+    gap = max(abs(r - oracle_res) for r in res) if oracle_res is not None else None
+    sample = (f"each step: one stock HOOI_ALS(X, 16^4, {sweeps}) call on the whole tensor "
+              f"(random init, {sweeps} sweeps, FP64), {os.cpu_count()} OpenMP threads + "
+              f"OpenBLAS threads; value = mean over the timed calls")
     out = {
         "impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": "ms",
-        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v, 1),
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v, 1),
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded Tucker tensor, generated in-process)",
-        "config": {"workload": "dense 96x96x96x96 FP32 Tucker(16^4) + N(0,1e-6), seed 1, "
-                               "upcast to FP64; reference HOOI_ALS, ranks 16^4"},
+        "config": _config(world),
+        "rel_err": res[-1] if res else None, "rel_err_oracle": oracle_res,
+        "rel_err_gap": gap, "target_met": bool(gap is not None and gap <= TARGET),
+        "step_ms": [round(x, 1) for x in t],
         "cpu_baseline": {"value": round(v, 1), "unit": "ms", "kind": "reference",
-                         "cores": os.cpu_count(),
-                         "sample": f"each step: one HOOI_ALS sweep ({one:.0f} ms median) "
-                                   f"x {sweeps} sweeps to converge"},
+                         "cores": os.cpu_count(), "cpu_model": _cpu_model(), "sample": sample},
         "e2e": {"value": round(v, 1), "unit": "ms", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }

@@ -139,6 +139,11 @@ inline void check_ctx(const dt_ctx *ctx) {
 
 bool is_device_ptr(const void *p);
 
+// Validates a dense shape: 1 <= ndim <= 16, every mode >= 1, and the element
+// count (so every product of modes) below 2^62.  Fails with DT_ERR_ARG naming
+// `who`.
+void check_shape(int ndim, const int64_t *shape, const char *who);
+
 // Raises a kernel's dynamic shared-memory limit to at least `bytes` on ctx's
 // device; the runtime is called only when the limit has to grow.
 void raise_smem_limit(dt_ctx *ctx, const void *kernel, size_t bytes);

@@ -21,6 +21,19 @@ std::string fmt(const char *f, ...) {
 void set_last_error(const std::string &msg) { g_last_error = msg; }
 void clear_last_error() { g_last_error.clear(); }
 
+void check_shape(int ndim, const int64_t *shape, const char *who) {
+    DT_CHECK_ARG(ndim >= 1 && ndim <= 16 && shape, "%s: bad ndim %d", who, ndim);
+    int64_t total = 1;
+    for (int i = 0; i < ndim; i++) {
+        DT_CHECK_ARG(shape[i] >= 1, "%s: shape[%d] = %lld must be >= 1", who, i,
+                     (long long)shape[i]);
+        DT_CHECK_ARG(shape[i] <= (int64_t(1) << 62) / total,
+                     "%s: the element count overflows at shape[%d] = %lld", who, i,
+                     (long long)shape[i]);
+        total *= shape[i];
+    }
+}
+
 bool is_device_ptr(const void *p) {
     if (!p) return false;
     cudaPointerAttributes attr;

@@ -6,13 +6,6 @@ using namespace dt;
 
 namespace {
 
-void check_shape(int ndim, const int64_t *shape, const char *who) {
-    DT_CHECK_ARG(ndim >= 1 && ndim <= 16 && shape, "%s: bad ndim %d", who, ndim);
-    for (int i = 0; i < ndim; i++)
-        DT_CHECK_ARG(shape[i] >= 1, "%s: shape[%d] = %lld must be >= 1", who, i,
-                     (long long)shape[i]);
-}
-
 struct ModeView {
     int64_t L, I, B;
 };

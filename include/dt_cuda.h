@@ -128,8 +128,10 @@ DT_API int dt_gram_f64(dt_ctx *ctx, const double *X, int ndim, const int64_t *sh
  * shape[mode] <= 1024.  The split-K partial tiles live in a fixed 16 MiB
  * `static __device__` array that every GPU loading this library holds until
  * exit.  The first call on a device looks the array up (cudaGetSymbolAddress):
- * make it before any stream capture.  Calls share the array, so calls whose
- * kernels overlap on the GPU race; serialise them. */
+ * make it before any stream capture.  The address is cached per device and
+ * CUDA context, so after a device reset the next call looks it up again.
+ * Calls share the array, so calls whose kernels overlap on the GPU race;
+ * serialise them. */
 DT_API int dt_gram_f64_noalloc(dt_ctx *ctx, const double *X, int ndim, const int64_t *shape,
                                int mode, double *G);
 

@@ -128,6 +128,21 @@ def hooi_als(X, ranks, max_iter, seed):
     return G, U, gn.value, xn.value
 
 
+def hooi_als_mt(X, ranks, max_iter, seed, threads=0):
+    """The reference's HOOI_ALS on `threads` OpenMP threads (0: all), as it
+    runs in production; the random start then varies run to run.
+    Returns (||G||, ||X||)."""
+    X = _f64(X)
+    gn = ctypes.c_double()
+    xn = ctypes.c_double()
+    s = _shape(X.shape)
+    r = _shape(ranks)
+    lib().ref_hooi_als_mt(_d(X), X.ndim, s.ctypes.data_as(_i64p), r.ctypes.data_as(_i64p),
+                          ctypes.c_int64(max_iter), ctypes.c_uint(seed), ctypes.c_int(threads),
+                          ctypes.byref(gn), ctypes.byref(xn))
+    return gn.value, xn.value
+
+
 def hooi_harness(X, ranks, max_iter, tol, U_init=None):
     """HOOI sweep built from the reference's Function::ttm + ALS_ with HOSVD
     init (U_init None) or the given factors, stopping on residual change < tol.

@@ -15,7 +15,11 @@
  *   ref_reduced_qr     -> Function::reduced_QR     template/function/matrix.tpp:86-101
  *   ref_inverse        -> Function::inverse        template/function/matrix.tpp:56-67
  *   ref_als            -> Algorithm::Tucker::ALS_  template/algorithm/tucker/hooi_als.tpp:7-34
- *   ref_hooi_als       -> Algorithm::Tucker::HOOI_ALS  hooi_als.tpp:64-123 (random init)
+ *   ref_hooi_als       -> Algorithm::Tucker::HOOI_ALS  hooi_als.tpp:64-123 (random init,
+ *                         drawn on one thread so the initial factors are reproducible)
+ *   ref_hooi_als_mt    -> the same call with every OpenMP thread the caller asks for,
+ *                         the reference's normal configuration (its randn then draws
+ *                         std::rand() from several threads, so the start varies)
  *   ref_hooi_harness   -> the HOOI_ALS sweep (hooi_als.tpp:94-114) composed from
  *                         Function::ttm + ALS_, with HOSVD init (Function::gram +
  *                         LAPACKE_dsyevd) and a fit-change stop rule; the
@@ -172,6 +176,25 @@ int ref_hooi_als(const double *X, int ndim, const int64_t *shape, const int64_t 
         if (U && U[n]) out(factors[(size_t)n], U[n]);
     if (g_norm) *g_norm = Function::fnorm<double>(core);
     if (x_norm) *x_norm = Function::fnorm<double>(A);
+    return 0;
+}
+
+/* The stock HOOI_ALS call on `threads` OpenMP threads (<= 0: all of them);
+ * OpenBLAS keeps its own thread pool.  This is how the reference runs in
+ * production, timed as the CPU baseline. */
+int ref_hooi_als_mt(const double *X, int ndim, const int64_t *shape, const int64_t *ranks,
+                    int64_t max_iter, unsigned seed, int threads, double *g_norm,
+                    double *x_norm) {
+    shape_t s = to_shape(ndim, shape);
+    shape_t R = to_shape(ndim, ranks);
+    auto A = dense_in(X, s);
+    const int saved = omp_get_max_threads();
+    omp_set_num_threads(threads > 0 ? threads : omp_get_num_procs());
+    std::srand(seed);
+    auto [core, factors] = Algorithm::Tucker::HOOI_ALS<double>(A, R, (size_t)max_iter);
+    if (g_norm) *g_norm = Function::fnorm<double>(core);
+    if (x_norm) *x_norm = Function::fnorm<double>(A);
+    omp_set_num_threads(saved);
     return 0;
 }
 

@@ -32,9 +32,12 @@ def oracle_sparse():
 def oracle_ref():
     from oracle import ref
     if not ref.available():
-        ref_dir = "/root/reference"
-        if os.path.isdir(ref_dir):
-            subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+        # oracle/Makefile builds it where the reference sources are present
+        # (REF, overridable by $DIANA_REF) and is a no-op elsewhere.
+        cmd = ["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"]
+        if os.environ.get("DIANA_REF"):
+            cmd.append("REF=" + os.environ["DIANA_REF"])
+        subprocess.run(cmd, check=True)
     if not ref.available():
         pytest.skip("compiled reference oracle (oracle/_ref/libdiana_ref.so) not available")
     return ref

@@ -92,7 +92,10 @@ def reference_runs() -> dict:
 
 
 def main():
-    ref_dir = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    # The reference checkout: the first argument, else $DIANA_REF, else the
+    # default location of the read-only checkout.
+    ref_dir = (sys.argv[1] if len(sys.argv) > 1
+               else os.environ.get("DIANA_REF", "/root/reference"))
     ka = known_answers(ref_dir)
     with open(os.path.join(HERE, "ref_known_answers.json"), "w") as f:
         json.dump(ka, f, indent=1)
