@@ -378,49 +378,87 @@ class Context:
         return U, fs.value, fi.value
 
     # -- batched ---------------------------------------------------------------
+    @staticmethod
+    def pack_batched(tensors, ranks, U0=None):
+        """Packs many small 3-way tensors for dt_hooi_batched: returns a dict
+        with the concatenated FP32 data ``X``, the ``shapes``/``ranks``
+        tables, the element offsets ``xoff``/``uoff``/``goff`` and (given
+        U0, a list of 3-lists of initial factors) the packed FP64 ``U``."""
+        count = len(tensors)
+        shapes = np.array([t.shape for t in tensors], dtype=np.int64).reshape(-1)
+        rk = np.array(ranks, dtype=np.int64).reshape(-1)
+        sizes = [int(np.prod(t.shape)) for t in tensors]
+        xoff = np.zeros(count, dtype=np.int64)
+        xoff[1:] = np.cumsum(sizes)[:-1]
+        X = np.empty(int(sum(sizes)), dtype=np.float32)
+        for t, x in enumerate(tensors):
+            X[xoff[t]:xoff[t] + sizes[t]] = np.asarray(x, dtype=np.float32).reshape(-1, order="F")
+        usz = [int(tensors[t].shape[n]) * int(ranks[t][n]) for t in range(count) for n in range(3)]
+        uoff = np.zeros(3 * count, dtype=np.int64)
+        uoff[1:] = np.cumsum(usz)[:-1]
+        gsz = [int(np.prod(r)) for r in ranks]
+        goff = np.zeros(count, dtype=np.int64)
+        goff[1:] = np.cumsum(gsz)[:-1]
+        out = {"count": count, "shapes": shapes, "ranks": rk, "X": X, "xoff": xoff,
+               "uoff": uoff, "goff": goff, "u_size": int(sum(usz)), "g_size": int(sum(gsz)),
+               "shape_list": [tuple(int(v) for v in t.shape) for t in tensors],
+               "rank_list": [tuple(int(v) for v in r) for r in ranks]}
+        if U0 is not None:
+            U = np.empty(out["u_size"])
+            for t in range(count):
+                for n in range(3):
+                    o = uoff[3 * t + n]
+                    U[o:o + usz[3 * t + n]] = np.asarray(U0[t][n], dtype=np.float64).reshape(
+                        -1, order="F")
+            out["U"] = U
+        return out
+
+    def hooi_batched_packed(self, packed, U, G, relerr, X=None, sweeps=10, inner_iters=5,
+                            block_threads=0):
+        """dt_hooi_batched on packed buffers (pack_batched): X (default
+        packed["X"]), U (in/out), G and relerr (out) may be numpy arrays (host,
+        staged by the library) or torch CUDA tensors (device-resident).
+        Returns the report dict."""
+        X = packed["X"] if X is None else X
+        self._bind(X, U, G, relerr)
+        xb = _Buf(X, dtype=np.float32, fortran=False)
+        ub = _Buf(U, fortran=False)
+        gb = _Buf(G, fortran=False)
+        eb = _Buf(relerr, fortran=False)
+        rep = _lib.BatchedReport()
+        _lib.check(self.lib.dt_hooi_batched(
+            self.h, packed["count"], _i64p(packed["shapes"]), _i64p(packed["ranks"]), xb.ptr,
+            _i64p(packed["xoff"]), sweeps, inner_iters, ub.ptr, _i64p(packed["uoff"]), gb.ptr,
+            _i64p(packed["goff"]), eb.ptr, block_threads, ctypes.byref(rep)))
+        return rep.as_dict()
+
     def hooi_batched(self, tensors, ranks, U0, sweeps=10, inner_iters=5, block_threads=0):
         """HOOI of many small 3-way tensors in one launch (dt_hooi_batched).
         tensors: list of FP32 arrays; ranks: list of 3-tuples; U0: list of
         3-lists of initial factors.  Returns (U, G, relerr, report)."""
-        count = len(tensors)
-        shapes = np.array([t.shape for t in tensors], dtype=np.int64).reshape(-1)
-        rk = np.array(ranks, dtype=np.int64).reshape(-1)
-        xs = [np.asfortranarray(t, dtype=np.float32).reshape(-1, order="F") for t in tensors]
-        xoff = np.zeros(count, dtype=np.int64)
-        xoff[1:] = np.cumsum([x.size for x in xs])[:-1]
-        X = np.concatenate(xs)
-        ublocks, uoff = [], []
-        o = 0
-        for t in range(count):
-            for n in range(3):
-                u = np.asfortranarray(U0[t][n], dtype=np.float64).reshape(-1, order="F")
-                ublocks.append(u)
-                uoff.append(o)
-                o += u.size
-        U = np.concatenate(ublocks)
-        uoff = np.array(uoff, dtype=np.int64)
-        gsz = [int(np.prod(r)) for r in ranks]
-        goff = np.zeros(count, dtype=np.int64)
-        goff[1:] = np.cumsum(gsz)[:-1]
-        G = np.zeros(int(sum(gsz)))
-        relerr = np.zeros(count)
-        rep = _lib.BatchedReport()
-        _lib.check(self.lib.dt_hooi_batched(
-            self.h, count, _i64p(shapes), _i64p(rk), X.ctypes.data, _i64p(xoff), sweeps,
-            inner_iters, U.ctypes.data, _i64p(uoff), G.ctypes.data, _i64p(goff),
-            relerr.ctypes.data, block_threads, ctypes.byref(rep)))
+        pk = self.pack_batched(tensors, ranks, U0)
+        U = pk["U"]
+        G = np.zeros(pk["g_size"])
+        relerr = np.zeros(pk["count"])
+        report = self.hooi_batched_packed(pk, U, G, relerr, sweeps=sweeps,
+                                          inner_iters=inner_iters, block_threads=block_threads)
+        return (*self.unpack_batched(pk, U, G), relerr, report)
+
+    @staticmethod
+    def unpack_batched(packed, U, G):
+        """Per-tensor factor lists and cores from packed U and G (host arrays)."""
+        U = np.asarray(U)
+        G = np.asarray(G)
         Uo, Go = [], []
-        for t in range(count):
+        for t, (shape, r) in enumerate(zip(packed["shape_list"], packed["rank_list"])):
             fac = []
             for n in range(3):
-                I, R = tensors[t].shape[n], ranks[t][n]
-                fac.append(np.reshape(U[uoff[3 * t + n]:uoff[3 * t + n] + I * R], (I, R), order="F"))
+                o = packed["uoff"][3 * t + n]
+                fac.append(np.reshape(U[o:o + shape[n] * r[n]], (shape[n], r[n]), order="F"))
             Uo.append(fac)
-            Go.append(np.reshape(G[goff[t]:goff[t] + gsz[t]], ranks[t], order="F"))
-        report = {"device_ms": rep.device_ms, "block_threads": rep.block_threads,
-                  "grid": rep.grid, "kernel_launches": rep.kernel_launches,
-                  "tune_ms": list(rep.tune_ms)}
-        return Uo, Go, relerr, report
+            o = packed["goff"][t]
+            Go.append(np.reshape(G[o:o + int(np.prod(r))], r, order="F"))
+        return Uo, Go
 
     # -- Summary profiler --------------------------------------------------------
     def summary_enable(self, on: bool = True):

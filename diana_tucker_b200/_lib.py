@@ -87,8 +87,16 @@ class BatchedReport(ctypes.Structure):
         ("block_threads", ctypes.c_int),
         ("grid", ctypes.c_int),
         ("kernel_launches", ctypes.c_int),
-        ("tune_ms", ctypes.c_double * 3),
+        ("pack", ctypes.c_int),
+        ("items", ctypes.c_int),
+        ("candidates_timed", ctypes.c_int),
+        ("tune_best_ms", ctypes.c_double),
+        ("tune_worst_ms", ctypes.c_double),
+        ("graph_reused", ctypes.c_int),
     ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 # (name, restype, argtypes)

@@ -33,6 +33,9 @@ struct dt_ctx {
     // of one sweep), reused by the next call with the same shapes, ranks and
     // options; released before the stream at dt_ctx_destroy.
     std::shared_ptr<void> hooi_plan_fp64, hooi_plan_mixed;
+    // The batched HOOI's tuned configurations, instantiated graphs and
+    // device-resident argument block (dt_hooi_batched).
+    std::shared_ptr<void> batched;
     // Summary profiler state (dt_summary_*; null until first enabled).
     std::shared_ptr<void> summary;
 };

@@ -214,6 +214,7 @@ int dt_ctx_destroy(dt_ctx *ctx) {
         if (ctx->stream) cudaStreamSynchronize(ctx->stream);
         ctx->hooi_plan_fp64.reset();
         ctx->hooi_plan_mixed.reset();
+        ctx->batched.reset();
         ctx->summary.reset();
         if (ctx->stream) cudaStreamSynchronize(ctx->stream);
         if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);

@@ -232,11 +232,17 @@ DT_API void dt_hooi_default_opts(dt_hooi_opts *opts);
 
 /* ---- batched dense HOOI ------------------------------------------------ */
 typedef struct {
-    double device_ms;    /* CUDA-event time of the graph launch */
-    int block_threads;   /* block size used (autotuned when 0 was requested) */
-    int grid;            /* persistent CTAs (resident CTAs per SM x SMs) */
+    double device_ms;     /* CUDA-event time of the graph launch */
+    int block_threads;    /* threads per CTA (autotuned when 0 was requested) */
+    int grid;             /* persistent CTAs (resident CTAs per SM x SMs) */
     int kernel_launches;
-    double tune_ms[3];   /* autotuner timings of 128 / 256 / 512 threads (0 if cached) */
+    int pack;             /* 0: one tensor per CTA; 1: tensors with largest mode
+                             <= 37 two to a CTA; 2: also those <= 21 four to a CTA */
+    int items;            /* work items (CTA-sized units) of the launch */
+    int candidates_timed; /* configurations the autotuner timed (0: cached) */
+    double tune_best_ms;  /* the autotuner's fastest and slowest sample times */
+    double tune_worst_ms;
+    int graph_reused;     /* 1: an instantiated graph of an earlier call replayed */
 } dt_batched_report;
 
 /* HOOI of `count` independent 3-way tensors in one persistent launch (CUDA
@@ -246,9 +252,13 @@ typedef struct {
  * FP64) at U + u_offsets[3t+n], overwritten with the result; the core goes to
  * G + g_offsets[t] and the relative error sqrt(1 - ||G||^2/||X||^2) to
  * relerr[t].  `sweeps` HOOI sweeps with `inner_iters` ALS_ steps per mode, in
- * FP64.  block_threads = 0 autotunes the block size on a sample of the batch
- * (cached per batch signature).  Batched form of Algorithm::Tucker::HOOI_ALS
- * (hooi_als.tpp:64-123); no reference counterpart for the batching. */
+ * FP64.  Tensors are ordered longest first and small ones may share a CTA.
+ * block_threads = 0 autotunes the block size and the packing on a sample of
+ * the batch (cached per batch signature); 128/256/512 fix the block size and
+ * pack the small tensors two and four to a CTA.  The instantiated graph is kept on the context and
+ * replayed by later calls with the same launch shape.  Batched form of
+ * Algorithm::Tucker::HOOI_ALS (hooi_als.tpp:64-123); no reference counterpart
+ * for the batching. */
 DT_API int dt_hooi_batched(dt_ctx *ctx, int count, const int64_t *shapes, const int64_t *ranks,
                            const float *X, const int64_t *x_offsets, int sweeps, int inner_iters,
                            double *U, const int64_t *u_offsets, double *G,
