@@ -598,6 +598,42 @@ class SpTensor:
                                             Y.ctypes.data))
         return Y
 
+    def _dense_args(self, M, idx):
+        """Factor pointers (J_m x I_m col-major, None for modes not in idx),
+        row counts and the mode list for dt_sp_ttmc_dense_f64 / mettmc."""
+        idx = [int(m) for m in idx]
+        keep, ptrs = [], (ctypes.c_void_p * self.ndim)()
+        J = np.zeros(self.ndim, dtype=np.int64)
+        for m in range(self.ndim):
+            if m in idx:
+                a = np.asfortranarray(M[m], dtype=np.float64)
+                if a.shape[1] != self.shape[m]:
+                    raise ValueError(f"M[{m}] must be J x {self.shape[m]}")
+                keep.append(a)
+                ptrs[m] = a.ctypes.data
+                J[m] = a.shape[0]
+        ids = (ctypes.c_int * max(1, len(idx)))(*idx)
+        out_shape = [int(J[m]) if m in idx else self.shape[m] for m in range(self.ndim)]
+        return keep, ptrs, J, ids, out_shape
+
+    def ttmc_dense(self, M, idx):
+        """Function::ttmc(SpTensor, M, idx, ...): A x_{m in idx} M[m] as a dense
+        column-major array (M[m] is J_m x I_m; modes outside idx keep I_m)."""
+        keep, ptrs, J, ids, out_shape = self._dense_args(M, idx)
+        Y = np.zeros(out_shape, order="F")
+        _lib.check(self.lib.dt_sp_ttmc_dense_f64(self.ctx.h, self.h, ptrs, _i64p(J), ids,
+                                                 len(list(idx)), Y.ctypes.data))
+        return Y
+
+    def mettmc(self, M, idx, level):
+        """Function::mettmc: the same result, the `level` least-compressing
+        modes (I_m / J_m) contracted densely after the sparse TTMc."""
+        keep, ptrs, J, ids, out_shape = self._dense_args(M, idx)
+        Y = np.zeros(out_shape, order="F")
+        _lib.check(self.lib.dt_sp_mettmc_f64(self.ctx.h, self.h, ptrs, _i64p(J), ids,
+                                             len(list(idx)), int(level), Y.ctypes.data))
+        return Y
+
     def hooi(self, R, max_sweeps, Ut0):
         Ut = [np.ascontiguousarray(u, dtype=np.float64).copy() for u in Ut0]
         ptrs = (ctypes.c_void_p * self.ndim)(*[a.ctypes.data for a in Ut])

@@ -152,6 +152,11 @@ _SIGS = [
                                        _vp]),
     ("dt_sp_hooi", ctypes.c_int, [_vp, _vp, c_i64p, ctypes.c_int, ctypes.POINTER(_vp), _vp,
                                   ctypes.POINTER(HooiReport)]),
+    ("dt_sp_ttmc_dense_f64", ctypes.c_int, [_vp, _vp, ctypes.POINTER(_vp), c_i64p,
+                                            ctypes.POINTER(ctypes.c_int), ctypes.c_int, _vp]),
+    ("dt_sp_mettmc_f64", ctypes.c_int, [_vp, _vp, ctypes.POINTER(_vp), c_i64p,
+                                        ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
+                                        _vp]),
     ("dt_tns_read", ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.POINTER(_vp),
                                    ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int64)]),
     ("dt_tns_parse", ctypes.c_int, [_vp, _vp, ctypes.c_int64, ctypes.POINTER(_vp),

@@ -161,6 +161,62 @@ inline void ttmc_mTL(const SpTensor<double> &A, const std::vector<Tensor<double>
                  "Function::ttmc_mTL");
 }
 
+// Sparse TTMc to a dense tensor (template/function/sp_tensor.tpp:16-192):
+// A x_{m in idx} M[m] with M[m] J_m x I_m; the other modes keep their extent.
+// The result carries `distribution` (world size 1: the whole tensor);
+// to_permu only chooses the reference's internal buffer order and does not
+// change the result.
+namespace detail {
+inline Tensor<double> sp_dense_out(const SpTensor<double> &A, const std::vector<Tensor<double>> &M,
+                                   const std::vector<size_t> &idx, Distribution *distribution,
+                                   std::vector<const double *> &mp, std::vector<int64_t> &J,
+                                   std::vector<int> &ids) {
+    shape_t out = A.shape();
+    mp.assign(A.ndim(), nullptr);
+    J.assign(A.ndim(), 0);
+    for (size_t m : idx) {
+        require(m < A.ndim() && m < M.size() && M[m].is_matrix() &&
+                    M[m].shape()[1] == A.shape()[m],
+                "Function::ttmc: M[m] must be J x I_m for every listed mode");
+        mp[m] = M[m].data();
+        J[m] = (int64_t)M[m].shape()[0];
+        out[m] = M[m].shape()[0];
+        ids.push_back((int)m);
+    }
+    return Tensor<double>(distribution, out, false);
+}
+}  // namespace detail
+
+inline Tensor<double> ttmc(const SpTensor<double> &A, const std::vector<Tensor<double>> &M,
+                           const std::vector<size_t> &idx, Distribution *distribution,
+                           bool to_permu) {
+    (void)to_permu;
+    std::vector<const double *> mp;
+    std::vector<int64_t> J;
+    std::vector<int> ids;
+    Tensor<double> ret = detail::sp_dense_out(A, M, idx, distribution, mp, J, ids);
+    diana::check(dt_sp_ttmc_dense_f64(diana::ctx(), A.handle(), mp.data(), J.data(), ids.data(),
+                                      (int)ids.size(), ret.data()),
+                 "Function::ttmc");
+    return ret;
+}
+
+// mettmc (sp_tensor.tpp:194-211): the same result, the `level` modes of idx
+// with the smallest I_m / J_m contracted by dense TTMs after the sparse TTMc.
+inline Tensor<double> mettmc(const SpTensor<double> &A, const std::vector<Tensor<double>> &M,
+                             const std::vector<size_t> &idx, Distribution *distribution,
+                             bool to_permu, size_t level) {
+    (void)to_permu;
+    std::vector<const double *> mp;
+    std::vector<int64_t> J;
+    std::vector<int> ids;
+    Tensor<double> ret = detail::sp_dense_out(A, M, idx, distribution, mp, J, ids);
+    diana::check(dt_sp_mettmc_f64(diana::ctx(), A.handle(), mp.data(), J.data(), ids.data(),
+                                  (int)ids.size(), (int)level, ret.data()),
+                 "Function::mettmc");
+    return ret;
+}
+
 inline double fnorm(const SpTensor<double> &A) {
     double out = 0.0;
     diana::check(dt_sp_fnorm(diana::ctx(), A.handle(), &out), "Function::fnorm");

@@ -25,78 +25,18 @@
 #include <vector>
 
 #include "dt_kernels.cuh"
+#include "dt_sparse.cuh"
 
 namespace dt {
 namespace {
 
-constexpr int MAXD = 8;
 constexpr int64_t CHUNK = 512;
 constexpr int FIB_CHUNK = 8;
 constexpr int64_t TASK_PACK_GRP = 128;
 constexpr int64_t TASK_PIECE_BATCHES = 64;
 
-struct ModeCopy {
-    int64_t nrows = 0;  // non-empty rows
-    DevMem rows;        // int32 [nrows]: row id of compact row k
-    // Row-kernel layout (orders other than 3): nonzeros sorted by this mode's
-    // index, cut into chunks of at most CHUNK nonzeros.
-    DevMem other;       // int32 [ndim-1][nnz]: the other modes' indices, in mode order
-    DevMem val;         // double [nnz]
-    DevMem rowptr;      // int64 [nrows+1]
-    int64_t nchunks = 0;
-    DevMem chunk_row;   // int32 [nchunks]: compact row of the chunk
-    DevMem chunk_beg;   // int64 [nchunks]
-    DevMem chunk_slot;  // int32 [nchunks]: -1 = write row directly, else partial slot
-    int64_t nslots = 0;
-    int64_t nmulti = 0;   // rows with more than one chunk
-    DevMem multi_row;     // int32 [nmulti]: compact row
-    DevMem multi_first;   // int32 [nmulti]: first partial slot
-    DevMem multi_count;   // int32 [nmulti]
-    // Fibre layout (3-way): nonzeros ordered by (row, fibre); a row's fibres,
-    // cut into sub-fibres of at most FIB_CHUNK nonzeros, come longest first
-    // and are padded with empty fibres to a multiple of 4 (a group).
-    int fmode = -1;       // fibre mode F; the element mode E is the remaining one
-    int64_t nfib = 0;     // fibre slots (4 per group)
-    DevMem e_idx;         // int32 [nnz]: i_E of each nonzero, in fibre order
-    DevMem e_val;         // double [nnz]
-    DevMem fib_idx;       // int32 [nfib]: i_F of each fibre slot (0 when empty)
-    DevMem fib_ptr;       // int32 [nfib+1]: its nonzeros
-    DevMem grp_row;       // int32 [nfib/4]: compact row of each group
-    DevMem grp_aux;       // int32 [nfib/4]: longest fibre | FB_ROW_END (last group of its row)
-    // Batches: int2 {first group, first nonzero} (+ an end entry); a batch is
-    // at most FB_GRP groups and FB_NZ nonzeros.  Tasks: int4 {first batch, end
-    // batch, partial slot or -1, 0}: packs of whole consecutive rows, or pieces
-    // of one long row, largest first.
-    int64_t nbatch = 0;
-    DevMem batches;
-    int64_t ntasks = 0;
-    DevMem tasks;
-    int64_t tslots = 0;
-    int64_t tmulti = 0;   // rows cut into several pieces
-    // Their partial rows are summed in two levels: segments of at most
-    // COMB_SEG consecutive pieces (tseg_first / tseg_count: piece slots), then
-    // each row's segments (tmulti_first / tmulti_count: segment indices).
-    DevMem tmulti_row, tmulti_first, tmulti_count;
-    int64_t nseg = 0;
-    DevMem tseg_first, tseg_count;
-};
-
-struct FactorSet {
-    const double *U[MAXD];  // transposed factors: row i of mode m at U[m] + i*R[m]
-    int R[MAXD];
-};
-
 }  // namespace
 }  // namespace dt
-
-struct dt_sptensor {
-    dt_ctx *ctx = nullptr;
-    int ndim = 0;
-    int64_t nnz = 0;
-    int64_t shape[dt::MAXD] = {};
-    double fnorm = 0.0;
-    std::vector<dt::ModeCopy> modes;
-};
 
 namespace dt {
 namespace {
@@ -1362,6 +1302,9 @@ void detach_sptensors(dt_ctx *ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (dt_sptensor *sp : ctx->sptensors) {
         sp->modes.clear();
+        sp->coo.idx.release();
+        sp->coo.val.release();
+        sp->dense_rows.clear();
         sp->ctx = nullptr;
     }
     ctx->sptensors.clear();
@@ -1447,6 +1390,15 @@ int dt_sptensor_create(dt_ctx *ctx, int64_t nnz, int ndim, const int64_t *const 
                                     ctx->stream));
             sp->modes.resize(ndim);
             for (int m = 0; m < ndim; m++) build_mode(ctx, sp, m, idx32, v.as<double>());
+            // The COO copy read by the general TTMc to a dense output.
+            sp->coo.idx.alloc(ctx, (size_t)ndim * nnz * sizeof(int32_t));
+            for (int m = 0; m < ndim; m++)
+                DT_CUDA(cudaMemcpyAsync(sp->coo.idx.as<int32_t>() + (int64_t)m * nnz,
+                                        idx32[m].get(), nnz * sizeof(int32_t),
+                                        cudaMemcpyDeviceToDevice, ctx->stream));
+            sp->coo.val.alloc(ctx, nnz * sizeof(double));
+            DT_CUDA(cudaMemcpyAsync(sp->coo.val.get(), v.ptr(), nnz * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, ctx->stream));
             DT_CUDA(cudaStreamSynchronize(ctx->stream));
             sp->fnorm = std::sqrt(h);
         } catch (...) {

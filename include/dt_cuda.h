@@ -298,6 +298,26 @@ DT_API int dt_sp_ttmc_mTL(dt_ctx *ctx, const dt_sptensor *sp, const double *cons
 DT_API int dt_sp_ttmc_rows(dt_ctx *ctx, const dt_sptensor *sp, const double *const *Ut,
                     const int64_t *R, int mode, double *Y);
 
+/* Y = A x_{m in idx} M_m as a dense column-major tensor: mode m has extent
+ * J[m] when m is listed in idx (nidx distinct modes, any order) and I_m
+ * otherwise.  M[m] is J[m] x I_m col-major (host or device; entries of
+ * modes outside idx are not read and may be NULL).  Duplicate coordinates add
+ * up; no floating-point atomics (rows of the kept modes are summed in a fixed
+ * order).  Replaces Function::ttmc(SpTensor, M, idx, distribution, to_permu)
+ * (sp_tensor.tpp:16-192, add_outer_product :419-450) at world size 1; the
+ * reference's to_permu only picks its internal buffer order, so it has no
+ * counterpart.  The grouping of the nonzeros by their kept coordinates is
+ * built on the first call per set of kept modes and kept on the tensor. */
+DT_API int dt_sp_ttmc_dense_f64(dt_ctx *ctx, const dt_sptensor *sp, const double *const *M,
+                                const int64_t *J, const int *idx, int nidx, double *Y);
+/* The same result by Function::mettmc (sp_tensor.tpp:194-211): the modes of
+ * idx sorted by I_m / J_m (integer quotient, ascending; ties keep the given
+ * order), the sparse TTMc of all but the first `level` of them, then
+ * Function::ttm (dt_ttm_f64's kernels) of those `level` modes in that order.
+ * 0 <= level <= nidx. */
+DT_API int dt_sp_mettmc_f64(dt_ctx *ctx, const dt_sptensor *sp, const double *const *M,
+                            const int64_t *J, const int *idx, int nidx, int level, double *Y);
+
 /* Sparse HOOI power sweeps: per mode L = Y_(n)^T U_n, U_n <- orth(Y_(n) L);
  * core G (P_{N-1} x R_{N-1} col-major = the core tensor col-major) after the
  * sweeps.  Ut holds the initial transposed factors on entry and the final

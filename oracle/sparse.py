@@ -117,3 +117,31 @@ def hooi(idx, vals, shape, R, max_iter, Ut0):
                       a.shape.ctypes.data_as(_i64p), a.R.ctypes.data_as(_i64p),
                       ctypes.c_int64(max_iter), Ut_p, G.ctypes.data_as(_dp), ctypes.byref(res))
     return G, Ut, res.value
+
+
+def ttmc_dense(idx, vals, shape, M, idx_modes):
+    """Function::ttmc(SpTensor, M, idx) at world size 1: A x_{m in idx_modes}
+    M[m] (M[m] J_m x I_m) as a dense column-major array."""
+    nd = len(shape)
+    idx_l = [np.ascontiguousarray(i, dtype=np.int64) for i in idx]
+    vals = np.ascontiguousarray(vals, dtype=np.float64)
+    shape_a = np.ascontiguousarray(shape, dtype=np.int64)
+    contract = (ctypes.c_int * nd)(*[1 if m in idx_modes else 0 for m in range(nd)])
+    Ms = [np.asfortranarray(M[m], dtype=np.float64) if m in idx_modes else np.zeros((1, 1))
+          for m in range(nd)]
+    J = np.ascontiguousarray([Ms[m].shape[0] if m in idx_modes else 0 for m in range(nd)],
+                             dtype=np.int64)
+    out_shape = [int(J[m]) if m in idx_modes else int(shape[m]) for m in range(nd)]
+    Y = np.zeros(out_shape, dtype=np.float64, order="F")
+    idx_p = (_i64p * nd)(*[i.ctypes.data_as(_i64p) for i in idx_l])
+    M_p = (_dp * nd)(*[m.ctypes.data_as(_dp) for m in Ms])
+    lib().orc_sp_ttmc_dense(ctypes.c_int64(vals.shape[0]), nd, idx_p, vals.ctypes.data_as(_dp),
+                            shape_a.ctypes.data_as(_i64p), M_p, J.ctypes.data_as(_i64p),
+                            contract, Y.ctypes.data_as(_dp))
+    return Y
+
+
+def mettmc_order(shape, J, idx_modes):
+    """The mode order of Function::mettmc (sp_tensor.tpp:198-200): idx sorted
+    by I_m / J_m (integer quotient) ascending; ties keep the given order."""
+    return sorted(idx_modes, key=lambda m: int(shape[m]) // int(J[m]))

@@ -20,6 +20,14 @@
  *   orc_sp_hooi        Sp_HOOI_ALS / Sp_TTMC_ALS_, template/algorithm/sp_tucker/
  *                      sp_hooi_als.tpp:48-118: per mode L = Y_(n)^T U_n,
  *                      U_n <- orth2(Y_(n) L); core G = mTR(N-1) after the sweeps.
+ *   orc_sp_ttmc_dense  Function::ttmc(SpTensor, M, idx, ...), sp_tensor.tpp:16-192,
+ *                      at world size 1 (one rank: the whole output is the local
+ *                      block and the ring has one step): every nonzero, in input
+ *                      order, is added by the recursion of add_outer_product
+ *                      (sp_tensor.tpp:419-450), from the highest mode down; a
+ *                      contracted mode m loops over the J_m entries of
+ *                      M_m(:, i_m) (M_m J_m x I_m column-major), a kept mode jumps
+ *                      to its index.  The output is column-major.
  *
  * Factors are passed TRANSPOSED as in the reference (sp_hooi_als.tpp:80):
  * Ut[m] is R_m x I_m column-major, so factor row i is Ut[m] + i*R_m.
@@ -192,6 +200,44 @@ int orc_sp_ttmc_mTL(int64_t nnz, int ndim, const int64_t *const *idx, const doub
     }
     free(pos);
     free(perm);
+    return 0;
+}
+
+/* One nonzero's contribution below mode `dim` (add_outer_product). */
+static void outer_add(double *data, const int64_t *stride, int dim, const int *contract,
+                      const double *const *M, const int64_t *J, const int64_t *index,
+                      double val) {
+    if (contract[dim]) {
+        const double *col = M[dim] + index[dim] * J[dim];
+        for (int64_t j = 0; j < J[dim]; j++) {
+            if (dim == 0)
+                data[j] += val * col[j];
+            else
+                outer_add(data + stride[dim] * j, stride, dim - 1, contract, M, J, index,
+                          val * col[j]);
+        }
+    } else if (dim == 0) {
+        data[index[0]] += val;
+    } else {
+        outer_add(data + stride[dim] * index[dim], stride, dim - 1, contract, M, J, index, val);
+    }
+}
+
+/* Y (column-major; mode m has extent J[m] if contract[m], else shape[m]). */
+int orc_sp_ttmc_dense(int64_t nnz, int ndim, const int64_t *const *idx, const double *vals,
+                      const int64_t *shape, const double *const *M, const int64_t *J,
+                      const int *contract, double *Y) {
+    int64_t stride[MAXD], total = 1;
+    for (int m = 0; m < ndim; m++) {
+        stride[m] = total;
+        total *= contract[m] ? J[m] : shape[m];
+    }
+    memset(Y, 0, (size_t)total * sizeof(double));
+    int64_t index[MAXD];
+    for (int64_t e = 0; e < nnz; e++) {
+        for (int m = 0; m < ndim; m++) index[m] = idx[m][e];
+        outer_add(Y, stride, ndim - 1, contract, M, J, index, vals[e]);
+    }
     return 0;
 }
 

@@ -116,6 +116,60 @@ int main(int argc, char **argv) {
         EXPECT(gn > 0 && gn <= an * (1 + 1e-12), "sparse ||G|| %.6g vs ||A|| %.6g", gn, an);
         EXPECT(Ut.size() == 3 && Ut[0].shape()[0] == 4 && Ut[0].shape()[1] == 40, "Ut shapes");
     }
+    // Function::ttmc / mettmc of a sparse tensor to a dense one, against the
+    // drop-in's dense Function::ttm chain on the densified tensor.
+    {
+        const size_t nnz = 300;
+        const size_t dims[3] = {12, 9, 7};
+        auto *dbf = new data_buffer<double>();
+        dbf->ndim = 3;
+        dbf->nnz = nnz;
+        dbf->dims = (size_t *)std::malloc(3 * sizeof(size_t));
+        for (int m = 0; m < 3; m++) dbf->dims[m] = dims[m];
+        dbf->index_lists = (size_t **)std::malloc(3 * sizeof(size_t *));
+        for (int m = 0; m < 3; m++) dbf->index_lists[m] = (size_t *)std::malloc(nnz * sizeof(size_t));
+        dbf->vals = (double *)std::malloc(nnz * sizeof(double));
+        srand(11);
+        Tensor<double> dense({dims[0], dims[1], dims[2]}, true);
+        for (size_t e = 0; e < nnz; e++) {
+            size_t lin = 0, st = 1;
+            for (int m = 0; m < 3; m++) {
+                dbf->index_lists[m][e] = (size_t)(std::rand() % dims[m]);
+                lin += dbf->index_lists[m][e] * st;
+                st *= dims[m];
+            }
+            dbf->vals[e] = (double)(std::rand() % 1000) / 100.0 - 5.0;
+            dense[lin] += dbf->vals[e];
+        }
+        SpTensor<double> A(dbf);
+        std::vector<Tensor<double>> M;
+        for (int m = 0; m < 3; m++) {
+            Tensor<double> Mm({(size_t)(3 + m), dims[m]}, false);
+            for (size_t i = 0; i < Mm.size(); i++) Mm[i] = std::sin(0.37 * (double)(i + 11 * m));
+            M.push_back(Mm);
+        }
+        auto *dist = new DistributionCartesianBlock({1, 1, 1}, mpi_rank());
+        auto Y = Function::ttmc(A, M, {2, 0}, dist, true);
+        auto Yd = Function::ttm(Function::ttm(dense, M[2], 2), M[0], 0);
+        EXPECT(Y.shape() == Yd.shape(), "ttmc shape");
+        double err = 0.0, mx = 0.0;
+        for (size_t i = 0; i < Yd.size(); i++) {
+            err = std::fmax(err, std::fabs(Y[i] - Yd[i]));
+            mx = std::fmax(mx, std::fabs(Yd[i]));
+        }
+        EXPECT(err <= 1e-12 * mx, "ttmc vs dense chain: %.3g", err / mx);
+        for (size_t level = 0; level <= 3; level++) {
+            auto Ym = Function::mettmc(A, M, {0, 1, 2}, dist, false, level);
+            auto Yf = Function::ttm(Function::ttm(Function::ttm(dense, M[0], 0), M[1], 1), M[2], 2);
+            double e2 = 0.0, m2 = 0.0;
+            for (size_t i = 0; i < Yf.size(); i++) {
+                e2 = std::fmax(e2, std::fabs(Ym[i] - Yf[i]));
+                m2 = std::fmax(m2, std::fabs(Yf[i]));
+            }
+            EXPECT(Ym.shape() == Yf.shape() && e2 <= 1e-12 * m2, "mettmc level %zu: %.3g", level,
+                   e2 / m2);
+        }
+    }
     // read_data on a small .tns file (1-based indices), then SpTensor from it.
     {
         const std::string tns = std::string(argv[1]) + ".tns";

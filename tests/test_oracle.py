@@ -237,3 +237,38 @@ def test_sparse_hooi_matches_dense_power_sweep(oracle_sparse):
     Gd = dense.core(X, U)
     assert abs(np.linalg.norm(G) - np.linalg.norm(Gd)) < 1e-11 * np.linalg.norm(Gd)
     assert abs(res - dense.residual(np.linalg.norm(vals), np.linalg.norm(Gd))) < 1e-11
+
+
+def _with_duplicates(idx, vals, seed):
+    """Repeats a few nonzeros (same coordinates, other values): the TTMc adds
+    duplicates up, as add_outer_product's += does."""
+    rng = np.random.default_rng(seed)
+    rep = rng.choice(len(vals), size=max(1, len(vals) // 5), replace=False)
+    idx = [np.concatenate([i, i[rep]]) for i in idx]
+    vals = np.concatenate([vals, rng.lognormal(0, 1, rep.size)])
+    return idx, vals
+
+
+@pytest.mark.parametrize("shape,modes", [((9, 7, 5), []), ((9, 7, 5), [0]), ((9, 7, 5), [2, 1]),
+                                         ((9, 7, 5), [0, 1, 2]), ((8, 6, 7, 5), [3, 1]),
+                                         ((8, 6, 7, 5), [0, 2, 3])])
+def test_sparse_ttmc_dense_vs_reference_ttm_chain(oracle_sparse, oracle_ref, shape, modes):
+    """orc_sp_ttmc_dense (Function::ttmc at world size 1) == the reference's own
+    Function::ttm applied to the densified tensor, one listed mode at a time."""
+    idx, vals, shape = _small_sparse(7, shape, 70)
+    idx, vals = _with_duplicates(idx, vals, 8)
+    rng = np.random.default_rng(9)
+    M = [np.asfortranarray(rng.standard_normal((3 + m, shape[m]))) for m in range(len(shape))]
+    Y = oracle_sparse.ttmc_dense(idx, vals, shape, M, modes)
+    Yd = _densify(idx, vals, shape)
+    for m in modes:
+        Yd = oracle_ref.ttm(Yd, M[m], m)
+    assert Y.shape == Yd.shape
+    np.testing.assert_allclose(Y, Yd, rtol=1e-12, atol=1e-12)
+
+
+def test_sparse_mettmc_order_is_the_reference_sort(oracle_sparse):
+    # I_m / J_m as integer quotients: 9/3 = 3, 7/4 = 1, 5/5 = 1, ascending,
+    # ties in the given order.
+    assert oracle_sparse.mettmc_order([9, 7, 5], [3, 4, 5], [0, 2, 1]) == [2, 1, 0]
+    assert oracle_sparse.mettmc_order([9, 7, 5], [3, 4, 5], [1, 2, 0]) == [1, 2, 0]
