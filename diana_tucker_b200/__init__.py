@@ -18,9 +18,10 @@ import numpy as np
 
 from . import _lib
 from ._lib import (DT_INIT_GIVEN, DT_INIT_HOSVD, DT_INIT_RANDN_LIBC, DT_PREC_BF16,
-                   DT_PREC_BF16X2, DT_PREC_FP64, DTError, HooiOpts, HooiReport)
+                   DT_PREC_BF16X2, DT_PREC_BF16XH, DT_PREC_FP64, DTError, HooiOpts, HooiReport)
 
 __all__ = ["Context", "SpTensor", "DTError", "DT_PREC_FP64", "DT_PREC_BF16", "DT_PREC_BF16X2",
+           "DT_PREC_BF16XH",
            "DT_INIT_RANDN_LIBC", "DT_INIT_HOSVD", "DT_INIT_GIVEN"]
 
 

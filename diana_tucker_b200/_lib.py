@@ -29,6 +29,7 @@ DT_INIT_GIVEN = 2
 DT_PREC_FP64 = 0
 DT_PREC_BF16 = 1
 DT_PREC_BF16X2 = 2
+DT_PREC_BF16XH = 3
 
 DT_MAX_HIST = 256
 

@@ -11,11 +11,13 @@
 // first so the non-contracted prefix (the TMA row dimension) stays long, and a
 // leaf's last contraction writes Y_(n) K-major for the Gram.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 
 #include "dt_hooi.cuh"
 #include "dt_kernels.cuh"
+#include "dt_leaf.cuh"
 #include "dt_tc_host.cuh"
 
 namespace dt {
@@ -41,8 +43,11 @@ struct MixedHooi {
     const float *X32 = nullptr;
     DevMem X32own, Xh, Xl;
     std::vector<DevMem> U;
-    DevMem S, work, flag, err, scal, Gs;
-    bool split = false;
+    DevMem S, work, flag, err, scal, Gs, lpart;
+    size_t lpart_doubles = 0;
+    bool split = false;   // intermediates, U and the Gram operands as hi + lo
+    bool xsplit = false;  // X itself as hi + lo (else X in BF16 hi only)
+    bool pair_gram_on = true;  // pair nodes: leaf Grams straight from the pair tensor
     DenseHooi helper;  // initial factors (same generators as the FP64 driver)
     LaunchTimer *xtimer = nullptr;
     SweepGraph *g_bf16 = nullptr, *g_split = nullptr;  // captured sweeps (or null)
@@ -156,14 +161,18 @@ struct MixedHooi {
                     om.sb[0] = 0;
                 }
             }
-            const bool from_x = xtimer && sh == Xh.as<__nv_bfloat16>();
+            const bool is_x = sh == Xh.as<__nv_bfloat16>();
+            const bool from_x = xtimer && is_x;
+            // X is read as hi + lo only when xsplit; every other operand, U and
+            // the output follow `split`.
+            const __nv_bfloat16 *a_lo = split && (!is_x || xsplit) ? sl : nullptr;
             if (from_x) xtimer->begin();
-            tc_ttm(ctx, sh, split ? sl : nullptr, L, cur.shape[m], B, U[m].as<double>(), R[m], om,
+            tc_ttm(ctx, sh, a_lo, L, cur.shape[m], B, U[m].as<double>(), R[m], om,
                    nxt.hi.as<__nv_bfloat16>(), split ? nxt.lo.as<__nv_bfloat16>() : nullptr,
-                   nullptr, err.as<int>());
+                   nullptr, err.as<int>(), split ? 1 : 0);
             if (from_x)
-                xtimer->end(((double)L * cur.shape[m] * B + (double)L * R[m] * B) * 2 *
-                                (split ? 2 : 1) +
+                xtimer->end((double)L * cur.shape[m] * B * 2 * (a_lo ? 2 : 1) +
+                            (double)L * R[m] * B * 2 * (split ? 2 : 1) +
                             (double)cur.shape[m] * R[m] * 8);
             cur = std::move(nxt);
             sh = cur.hi.as<__nv_bfloat16>();
@@ -179,15 +188,60 @@ struct MixedHooi {
         const __nv_bfloat16 *yh = Y.hi.as<__nv_bfloat16>();
         const __nv_bfloat16 *yl = split ? Y.lo.as<__nv_bfloat16>() : nullptr;
         tc_gram(ctx, yh, yl, I[n], K, S.as<double>(), err.as<int>());
-        subspace_iter(ctx, S.as<double>(), I[n], U[n].as<double>(), R[n], opts.inner_iters,
-                      work.as<double>(), flag.as<int>());
+        leaf_subspace(n, I[n], nullptr);
         if (n == N - 1)
             core_rows(ctx, yh, yl, I[n], K, U[n].as<double>(), R[n], Gs.as<double>(),
                       scal.as<double>() + 1);
     }
 
+    // Pair node {p, p + 1} of the tree whose leaves take their Grams from the
+    // pair tensor T itself (dt_leaf.cu): T's modes p, p+1 keep I, the others
+    // are contracted to R.
+    bool pair_ok(int p, const int64_t *shape) const {
+        int64_t nc = 1;
+        for (int k = 0; k < N; k++)
+            if (k != p && k != p + 1) nc *= shape[k];
+        return pair_gram_on && nc <= (int64_t(1) << 31) &&
+               pair_gram_supported(shape[p], shape[p + 1], R[p + 1]) &&
+               pair_gram_supported(shape[p], shape[p + 1], R[p]);
+    }
+
+    void pair(int p, const __nv_bfloat16 *Th, const __nv_bfloat16 *Tl, const int64_t *shape) {
+        const int q = p + 1;
+        int64_t clo = 1, chi = 1;
+        for (int k = 0; k < p; k++) clo *= shape[k];
+        for (int k = q + 1; k < N; k++) chi *= shape[k];
+        const int64_t np = shape[p], nq = shape[q];
+        const int64_t sp = clo, sq = clo * np, chs = clo * np * nq, nc = clo * chi;
+        // Leaf p: T x_q U_q^T, then leaf q with the new U_p.  The sweep's
+        // ||G||^2 = trace(U^T S U) of the last mode.
+        pair_gram(ctx, Th, Tl, np, nq, sp, sq, clo, chs, nc, 0, U[q].as<double>(), R[q],
+                  lpart.as<double>(), lpart_doubles, S.as<double>());
+        leaf_subspace(p, np, nullptr);
+        pair_gram(ctx, Th, Tl, np, nq, sp, sq, clo, chs, nc, 1, U[p].as<double>(), R[p],
+                  lpart.as<double>(), lpart_doubles, S.as<double>());
+        leaf_subspace(q, nq, q == N - 1 ? scal.as<double>() + 1 : nullptr);
+    }
+
+    // U_n <- orth(S^inner U_n) for the Gram S of mode n (size n_n); with g2,
+    // trace(U_n^T S U_n) is written there.
+    void leaf_subspace(int n, int64_t nn, double *g2) {
+        if (subspace_small_supported(nn, R[n])) {
+            subspace_small(ctx, S.as<double>(), nn, U[n].as<double>(), R[n], opts.inner_iters,
+                           flag.as<int>(), g2);
+            return;
+        }
+        subspace_iter(ctx, S.as<double>(), nn, U[n].as<double>(), R[n], opts.inner_iters,
+                      work.as<double>(), flag.as<int>());
+        if (g2) quad_trace(ctx, S.as<double>(), nn, U[n].as<double>(), R[n], g2);
+    }
+
     void node(int lo, int hi, const __nv_bfloat16 *Th, const __nv_bfloat16 *Tl,
               const int64_t *shape) {
+        if (hi - lo == 2 && pair_ok(lo, shape)) {
+            pair(lo, Th, Tl, shape);
+            return;
+        }
         const int mid = (lo + hi + 1) / 2;  // [0,3) -> [0,2) + [2,3): long TMA rows
         for (int side = 0; side < 2; side++) {
             const int clo = side == 0 ? lo : mid, chi = side == 0 ? mid : hi;
@@ -205,7 +259,7 @@ struct MixedHooi {
     }
 
     void sweep() {
-        node(0, N, Xh.as<__nv_bfloat16>(), split ? Xl.as<__nv_bfloat16>() : nullptr, I);
+        node(0, N, Xh.as<__nv_bfloat16>(), split && xsplit ? Xl.as<__nv_bfloat16>() : nullptr, I);
     }
 
     // 2 |X| R per X pass: each half of the tree first contracts its highest
@@ -234,8 +288,12 @@ struct MixedHooi {
         const int64_t launches0 = ctx->launches;
         LaunchTimer timer(ctx, opts.profile != 0);
         xtimer = &timer;
-        const bool want_split =
-            opts.precision == DT_PREC_BF16X2 || opts.refine_sweeps > 0;
+        // Whether X itself is kept as hi + lo: the split sweeps of DT_PREC_BF16X2
+        // and of DT_PREC_BF16's refinement read both halves; DT_PREC_BF16XH
+        // reads X in BF16 only (its intermediates, U and Grams are split).
+        const bool want_split = opts.precision == DT_PREC_BF16X2 ||
+                                (opts.precision == DT_PREC_BF16 && opts.refine_sweeps > 0);
+        xsplit = want_split;
         DT_CUDA(cudaEventRecord(ctx->ev_start, ctx->stream));
         if (dtype == DT_F32) {
             X32 = static_cast<const float *>(X);
@@ -274,7 +332,7 @@ struct MixedHooi {
         double prev = -1.0, res = 0.0;
         int sweeps = 0, bf16_done = 0, split_done = 0;
         const bool refine_mode = opts.precision == DT_PREC_BF16;
-        split = opts.precision == DT_PREC_BF16X2;
+        split = opts.precision == DT_PREC_BF16X2 || opts.precision == DT_PREC_BF16XH;
         for (int it = 0; it < opts.max_sweeps; it++) {
             if (!split && refine_mode && opts.refine_sweeps > 0 &&
                 it >= opts.max_sweeps - opts.refine_sweeps) {
@@ -285,7 +343,8 @@ struct MixedHooi {
                 // Counted work: the sweep's two passes over X (3 products per
                 // element and rank with split operands).
                 SummaryScope sc(ctx, split ? "HOOI sweep (BF16 split)" : "HOOI sweep (BF16)",
-                                x_pass_flop() * (split ? 3 : 1), 2.0 * xsize * (split ? 4 : 2));
+                                x_pass_flop() * (split ? (xsplit ? 3 : 2) : 1),
+                                2.0 * xsize * (split && xsplit ? 4 : 2));
                 SweepGraph *gr = split ? g_split : g_bf16;
                 if (gr && !opts.profile)
                     gr->run(ctx, [&] { sweep(); });
@@ -305,8 +364,8 @@ struct MixedHooi {
             if (rep && it < DT_MAX_HIST) rep->res_hist[it] = res;
             sweeps = it + 1;
             if (opts.verbose)
-                fprintf(stderr, "[dt_hooi bf16%s] sweep %d  residual = %.12e\n", split ? "x2" : "",
-                        it + 1, res);
+                fprintf(stderr, "[dt_hooi bf16%s] sweep %d  residual = %.12e\n",
+                        split ? (xsplit ? "x2" : "xh") : "", it + 1, res);
             const double delta = prev >= 0 ? std::fabs(res - prev) : 1e300;
             prev = res;
             if (!split) {
@@ -405,19 +464,19 @@ struct MixedHooi {
 
 // The mixed driver's buffers and captured sweeps (one graph per precision).
 struct MixedPlan {
-    int N, inner;
+    int N, inner, precision;
     int64_t I[16], R[16];
     MixedHooi h;
     SweepGraph g_bf16, g_split;
     MixedPlan(int n, const int64_t *shape, const int64_t *ranks, const dt_hooi_opts &o)
-        : N(n), inner(o.inner_iters) {
+        : N(n), inner(o.inner_iters), precision(o.precision) {
         for (int m = 0; m < n; m++) {
             I[m] = shape[m];
             R[m] = ranks[m];
         }
     }
     bool matches(int n, const int64_t *shape, const int64_t *ranks, const dt_hooi_opts &o) const {
-        if (n != N || o.inner_iters != inner) return false;
+        if (n != N || o.inner_iters != inner || o.precision != precision) return false;
         for (int m = 0; m < n; m++)
             if (shape[m] != I[m] || ranks[m] != R[m]) return false;
         return true;
@@ -429,7 +488,8 @@ struct MixedPlan {
 void hooi_dense_lowprec(dt_ctx *ctx, const void *X, int dtype, int ndim, const int64_t *shape,
                         const int64_t *ranks, const dt_hooi_opts &opts, double *G,
                         double *const *U, dt_hooi_report *report) {
-    DT_CHECK_ARG(opts.precision == DT_PREC_BF16 || opts.precision == DT_PREC_BF16X2,
+    DT_CHECK_ARG(opts.precision == DT_PREC_BF16 || opts.precision == DT_PREC_BF16X2 ||
+                     opts.precision == DT_PREC_BF16XH,
                  "unknown precision %d", opts.precision);
     DT_CHECK_ARG(opts.init != DT_INIT_HOSVD,
                  "the tensor-core HOOI starts from random or given factors, not HOSVD");
@@ -470,6 +530,20 @@ void hooi_dense_lowprec(dt_ctx *ctx, const void *X, int dtype, int ndim, const i
         h.err.alloc(ctx, sizeof(int));
         h.scal.alloc(ctx, 4 * sizeof(double));
         h.Gs.alloc(ctx, prod(ranks, ndim) * sizeof(double));
+        // Partial Grams of the pair nodes' leaves (the largest pair of the tree).
+        {
+            // DT_DISABLE_PAIR_GRAM=1 forms every Y_(n) and its Gram instead.
+            const char *e = std::getenv("DT_DISABLE_PAIR_GRAM");
+            h.pair_gram_on = !(e && e[0] == '1');
+        }
+        for (int p = 0; p + 1 < ndim; p++) {
+            int64_t nc = 1;
+            for (int k = 0; k < ndim; k++)
+                if (k != p && k != p + 1) nc *= ranks[k];
+            h.lpart_doubles = std::max(h.lpart_doubles,
+                                       pair_gram_scratch_doubles(shape[p], shape[p + 1], nc));
+        }
+        h.lpart.alloc(ctx, h.lpart_doubles * sizeof(double));
         h.g_bf16 = &plan->g_bf16;
         h.g_split = &plan->g_split;
         ctx->hooi_plan_mixed = plan;

@@ -71,13 +71,15 @@ __device__ __forceinline__ void tmem_ld_half(uint32_t taddr, float (&v)[JH]) {
     }
 }
 
-// JP: padded output width (16 or 32); SPLIT: hi+lo operands; FOLDED: the
+// JP: padded output width (16 or 32); BSPLIT: U as hi + lo (B = [U_hi | U_lo],
+// N = 2 JP); ASPLIT: X as hi + lo too (a second MMA X_lo U_hi); FOLDED: the
 // output is the folded tensor Y[l, j, b] (else a general OutMap).
-template <int JP, bool SPLIT, bool FOLDED>
+template <int JP, bool BSPLIT, bool ASPLIT, bool FOLDED>
 __global__ void __launch_bounds__(TTM_THREADS, 1)
     tc_ttm_kernel(const __grid_constant__ CUtensorMap map_hi,
                   const __grid_constant__ CUtensorMap map_lo, const TcTtmArgs a) {
-    constexpr int NPAD = SPLIT ? 2 * JP : JP;
+    static_assert(BSPLIT || !ASPLIT, "a split X needs a split U");
+    constexpr int NPAD = BSPLIT ? 2 * JP : JP;
     constexpr int JH = JP / 2;  // columns per epilogue warp
     extern __shared__ uint8_t smem_raw[];
     uint8_t *sm = align1024(smem_raw);
@@ -86,7 +88,7 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
     const uint32_t b_bytes = (uint32_t)a.kchunks * NPAD * 128;
     uint8_t *Abase = sm + ((b_bytes + 1023) & ~1023u);  // stages
     const uint32_t a_one = (uint32_t)a.kchunks * KC_BYTES;
-    const uint32_t stage_bytes = a_one * (SPLIT ? 2 : 1);
+    const uint32_t stage_bytes = a_one * (ASPLIT ? 2 : 1);
     uint64_t *bars = reinterpret_cast<uint64_t *>(Abase + (size_t)S * stage_bytes);
     uint64_t *full = bars, *empty = bars + S, *tfull = bars + 2 * S, *tempty = bars + 2 * S + 2;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * S + 4);
@@ -136,7 +138,7 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
     if (warp == 0) {
         if (lane == 0) {
             prefetch_tmap(&map_hi);
-            if (SPLIT) prefetch_tmap(&map_lo);
+            if (ASPLIT) prefetch_tmap(&map_lo);
             int64_t k = 0;
             bool ok = true;
             for (int64_t tile = blockIdx.x; tile < a.ntiles && ok; tile += gridDim.x, k++) {
@@ -149,7 +151,7 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
                     const int r0 = (int)(tile * 128);
                     for (int kc = 0; kc < a.kchunks; kc++) {
                         tma_load_2d(st + kc * KC_BYTES, &map_hi, &full[s], kc * KC_ELEMS, r0);
-                        if (SPLIT)
+                        if (ASPLIT)
                             tma_load_2d(st + a_one + kc * KC_BYTES, &map_lo, &full[s],
                                         kc * KC_ELEMS, r0);
                     }
@@ -160,7 +162,7 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
                         for (int h = 0; h < 2; h++) {
                             uint8_t *d = st + kc * KC_BYTES + h * (KC_BYTES / 2);
                             tma_load_3d(d, &map_hi, &full[s], l0 + h * 64, kc * KC_ELEMS, (int)b);
-                            if (SPLIT)
+                            if (ASPLIT)
                                 tma_load_3d(d + a_one, &map_lo, &full[s], l0 + h * 64,
                                             kc * KC_ELEMS, (int)b);
                         }
@@ -201,7 +203,7 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
                     const uint64_t bd =
                         sdesc(bt + (uint32_t)kc * NPAD * 128 + sub * 32, 16, 1024, kSwizzle128B);
                     umma_bf16(d, ad, bd, id_full, ks > 0 ? 1u : 0u);
-                    if (SPLIT) umma_bf16(d, adl, bd, id_half, 1u);
+                    if (ASPLIT) umma_bf16(d, adl, bd, id_half, 1u);
                 }
                 umma_commit(&empty[s]);
                 umma_commit(&tfull[acc]);
@@ -228,7 +230,7 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
                 tmem_base + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(acc * NPAD + j0);
             float v[JH];
             tmem_ld_half<JH>(taddr, v);
-            if (SPLIT) {
+            if (BSPLIT) {
                 float w[JH];
                 tmem_ld_half<JH>(taddr + JP, w);
                 tmem_wait_ld();
@@ -577,7 +579,7 @@ bool tc_ttm_supported(int64_t L, int64_t I, int64_t B, int64_t J) {
 
 void tc_ttm(dt_ctx *ctx, const __nv_bfloat16 *Xh, const __nv_bfloat16 *Xl, int64_t L, int64_t I,
             int64_t B, const double *U, int64_t J, const OutMap &om, __nv_bfloat16 *out_hi,
-            __nv_bfloat16 *out_lo, float *out_f32, int *err) {
+            __nv_bfloat16 *out_lo, float *out_f32, int *err, int usplit) {
     DT_CHECK_ARG(tc_ttm_supported(L, I, B, J), "tc_ttm: unsupported shape L=%lld I=%lld J=%lld",
                  (long long)L, (long long)I, (long long)J);
     TcTtmArgs a{};
@@ -588,7 +590,8 @@ void tc_ttm(dt_ctx *ctx, const __nv_bfloat16 *Xh, const __nv_bfloat16 *Xl, int64
     a.J = (int)J;
     a.Jpad = pad16((int)J);
     a.split = Xl != nullptr;
-    a.Npad = a.split ? 2 * a.Jpad : a.Jpad;
+    const bool bsplit = usplit < 0 ? a.split : (usplit != 0 || a.split);
+    a.Npad = bsplit ? 2 * a.Jpad : a.Jpad;
     a.kchunks = (int)((I + KC_ELEMS - 1) / KC_ELEMS);
     a.ksteps = (int)((I + 15) / 16);
     a.nmb = a.kmajor ? (B + 127) / 128 : (L + 127) / 128;
@@ -633,13 +636,23 @@ void tc_ttm(dt_ctx *ctx, const __nv_bfloat16 *Xh, const __nv_bfloat16 *Xl, int64
         smem_limit(ctx, kernel, smem);
         DT_LAUNCH_PDL(ctx, kernel, grid, TTM_THREADS, smem, mh, ml, a);
     };
-    if (a.Jpad == 16) {
-        if (a.split) folded ? go(tc_ttm_kernel<16, true, true>) : go(tc_ttm_kernel<16, true, false>);
-        else folded ? go(tc_ttm_kernel<16, false, true>) : go(tc_ttm_kernel<16, false, false>);
-    } else {
-        if (a.split) folded ? go(tc_ttm_kernel<32, true, true>) : go(tc_ttm_kernel<32, true, false>);
-        else folded ? go(tc_ttm_kernel<32, false, true>) : go(tc_ttm_kernel<32, false, false>);
-    }
+#define DT_TTM_GO(JP)                                                                    \
+    do {                                                                                 \
+        if (a.split)                                                                     \
+            folded ? go(tc_ttm_kernel<JP, true, true, true>)                             \
+                   : go(tc_ttm_kernel<JP, true, true, false>);                           \
+        else if (bsplit)                                                                 \
+            folded ? go(tc_ttm_kernel<JP, true, false, true>)                            \
+                   : go(tc_ttm_kernel<JP, true, false, false>);                          \
+        else                                                                             \
+            folded ? go(tc_ttm_kernel<JP, false, false, true>)                           \
+                   : go(tc_ttm_kernel<JP, false, false, false>);                         \
+    } while (0)
+    if (a.Jpad == 16)
+        DT_TTM_GO(16);
+    else
+        DT_TTM_GO(32);
+#undef DT_TTM_GO
 }
 
 bool tc_gram_supported(int64_t I, int64_t K) {

@@ -49,11 +49,13 @@ struct TcGramArgs {
 
 bool tc_ttm_supported(int64_t L, int64_t I, int64_t B, int64_t J);
 // Y = X x_n U^T on the tensor cores, X seen as [l, i, b] with strides
-// (1, L, L*I).  Xl may be NULL (BF16 only); out_lo may be NULL; with out_f32
-// non-NULL the result is written in FP32 instead of BF16.
+// (1, L, L*I).  Xl may be NULL (X in BF16 only); out_lo may be NULL; with
+// out_f32 non-NULL the result is written in FP32 instead of BF16.  U is split
+// into hi + lo when X is (or usplit > 0 with a BF16-only X: one MMA of
+// X_hi [U_hi | U_lo]); usplit < 0 follows X.
 void tc_ttm(dt_ctx *ctx, const __nv_bfloat16 *Xh, const __nv_bfloat16 *Xl, int64_t L, int64_t I,
             int64_t B, const double *U, int64_t J, const OutMap &om, __nv_bfloat16 *out_hi,
-            __nv_bfloat16 *out_lo, float *out_f32, int *err);
+            __nv_bfloat16 *out_lo, float *out_f32, int *err, int usplit = -1);
 
 bool tc_gram_supported(int64_t I, int64_t K);
 // S (I x I, FP64) = Y Y^T for the K-major BF16 Y (I rows of K); with Yl the

@@ -58,6 +58,8 @@ extern "C" {
 #define DT_PREC_FP64 0   /* FP64 CUDA-core kernels throughout (the drop-in) */
 #define DT_PREC_BF16 1   /* tcgen05 BF16 x BF16 -> FP32 TTM chain and Gram */
 #define DT_PREC_BF16X2 2 /* tcgen05 with split hi+lo BF16 operands (~2^-16) */
+#define DT_PREC_BF16XH 3 /* X rounded once to BF16 (2 bytes per element per pass);
+                            U, the intermediates and the Grams split hi+lo */
 
 typedef struct dt_ctx dt_ctx;
 

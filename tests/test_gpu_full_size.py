@@ -67,11 +67,12 @@ def test_dense_96x4_fp64_vs_reference(ctx, x96):
         assert dense.principal_angle_max(U[n], Uref[n]) <= 1e-8, n
 
 
-def test_dense_96x4_mixed_vs_reference(ctx, x96):
-    from diana_tucker_b200 import DT_PREC_BF16X2
+@pytest.mark.parametrize("prec", ["BF16X2", "BF16XH"])
+def test_dense_96x4_mixed_vs_reference(ctx, x96, prec):
+    import diana_tucker_b200 as dtb
     ref, Uref = _ref_96x4()
     G, U, rep = ctx.hooi_dense(x96, (16,) * 4, init="randn", seed=1, max_sweeps=30, tol=1e-9,
-                               precision=DT_PREC_BF16X2, inner_iters=2)
+                               precision=getattr(dtb, "DT_PREC_" + prec), inner_iters=2)
     assert rep["sweeps"] < 30
     assert abs(rep["residual"] - ref["residual"]) <= 1e-6
     assert abs(rep["g_norm"] - ref["g_norm"]) <= 1e-6 * ref["g_norm"]
