@@ -127,9 +127,26 @@ def warm_hooi(ctx, X, shape, ranks, model, *, max_sweeps=60, tol=1e-12):
     return U, rep, info
 
 
-def evaluate(ctx, seeds, model, *, max_sweeps=60, log=None):
+def ablation_model(model, kind: str, seed: int = 11):
+    """The same sketch-and-refine pipeline with another decoder, to show what
+    training adds: kind "random" -- an untrained decoder (orthonormalised
+    Gaussian n x k); kind "chebyshev" -- a fixed orthonormal basis of the first
+    k Chebyshev polynomials on n points of [-1, 1], chosen without looking at
+    any data.  The screening floor is the trained model's."""
+    n, k = model["D"].shape
+    if kind == "random":
+        D = np.linalg.qr(np.random.default_rng(seed).standard_normal((n, k)))[0]
+    elif kind == "chebyshev":
+        D = np.linalg.qr(np.polynomial.chebyshev.chebvander(np.linspace(-1.0, 1.0, n), k - 1))[0]
+    else:
+        raise ValueError(kind)
+    return dict(model, D=np.asfortranarray(D), kind=kind)
+
+
+def evaluate(ctx, seeds, model, *, max_sweeps=60, log=None, models=None):
     """Held-out comparison: sweeps and time to the converged FP64 residual +
-    1e-6, HOSVD init versus the learned warm start."""
+    1e-6 (and + 1e-9), HOSVD init versus the learned warm start, and versus
+    the pipeline with the decoders of `models` (name -> model; ablations)."""
     fam = model["family"]
     n, r = fam["size"], fam["rank"]
     shape, ranks = [n] * 3, [r] * 3
@@ -145,19 +162,46 @@ def evaluate(ctx, seeds, model, *, max_sweeps=60, log=None):
         # Residual of the HOSVD start itself (evaluation only).
         _, _, rep_h0 = ctx.hooi_dense(X, ranks, init="hosvd", max_sweeps=0, precision=DT_PREC_FP64,
                                       want_core=False, want_factors=False, shape=shape)
-        conv = min(rep_h["residual"], rep_w["residual"])
+        extra = {}
+        for name, m in (models or {}).items():
+            t0 = time.time()
+            _, rep_a, info_a = warm_hooi(ctx, X, shape, ranks, m, max_sweeps=max_sweeps)
+            extra[name] = (rep_a, info_a, time.time() - t0)
+        conv = min([rep_h["residual"], rep_w["residual"]] +
+                   [e[0]["residual"] for e in extra.values()])
         target = conv + 1e-6
-        r_w0 = float(np.sqrt(max(0.0, 1.0 - info["fit_init"])))
-        if info["fallback"]:
-            r_w0 = rep_h0["residual"]
+        strict = conv + 1e-9
+
+        def start_res(info_x):
+            if info_x["fallback"]:
+                return rep_h0["residual"]
+            return float(np.sqrt(max(0.0, 1.0 - info_x["fit_init"])))
+
+        r_w0 = start_res(info)
         sh = first_reaching(rep_h0["residual"], rep_h["res_hist"], target)
         sw = first_reaching(r_w0, rep_w["res_hist"], target)
-        rows.append(dict(seed=s, target=target, sweeps_hosvd=sh, sweeps_warm=sw,
-                         wall_hosvd_s=th, wall_warm_s=tw, **info))
+        row = dict(seed=s, target=target, sweeps_hosvd=sh, sweeps_warm=sw,
+                   sweeps_hosvd_strict=first_reaching(rep_h0["residual"], rep_h["res_hist"],
+                                                      strict),
+                   sweeps_warm_strict=first_reaching(r_w0, rep_w["res_hist"], strict),
+                   wall_hosvd_s=th, wall_warm_s=tw, **info)
+        for name, (rep_a, info_a, ta) in extra.items():
+            ra0 = start_res(info_a)
+            row[f"sweeps_{name}"] = first_reaching(ra0, rep_a["res_hist"], target)
+            row[f"sweeps_{name}_strict"] = first_reaching(ra0, rep_a["res_hist"], strict)
+            row[f"wall_{name}_s"] = ta
+            row[f"fit_init_{name}"] = info_a["fit_init"]
+            row[f"fallback_{name}"] = info_a["fallback"]
+        rows.append(row)
         if log:
             log(f"eval seed {s}: hosvd {sh} sweeps, warm {sw} sweeps, fit_init {info['fit_init']:.6f}"
                 f"{' (fallback)' if info['fallback'] else ''}")
     return rows
+
+
+def _mean(rows, key):
+    v = [r[key] for r in rows if r.get(key) is not None]
+    return float(np.mean(v)) if v else None
 
 
 def summarize(rows):
@@ -166,7 +210,20 @@ def summarize(rows):
     sw = np.array([r["sweeps_warm"] for r in ok], dtype=float)
     mh = float(sh.mean()) if len(ok) else None
     mw = float(sw.mean()) if len(ok) else None
+    out = {}
+    names = sorted({k[len("fit_init_"):] for r in rows for k in r if k.startswith("fit_init_")})
+    for name in names:
+        wall = _mean(rows, f"wall_{name}_s")
+        out[name] = dict(mean_sweeps=_mean(rows, f"sweeps_{name}"),
+                         mean_sweeps_strict=_mean(rows, f"sweeps_{name}_strict"),
+                         mean_fit_init=_mean(rows, f"fit_init_{name}"),
+                         fallback_rate=_mean(rows, f"fallback_{name}"),
+                         mean_wall_ms=1e3 * wall if wall is not None else None)
     return dict(
+        mean_sweeps_hosvd_strict=_mean(rows, "sweeps_hosvd_strict"),
+        mean_sweeps_warm_strict=_mean(rows, "sweeps_warm_strict"),
+        mean_fit_init_warm=_mean(rows, "fit_init"),
+        ablation=out,
         tensors=len(rows),
         reached=len(ok),
         mean_sweeps_hosvd=mh,

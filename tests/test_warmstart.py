@@ -128,3 +128,20 @@ def test_off_family_tensor_falls_back_to_hosvd(ctx, small_model):
     assert info["screened"] and info["fallback"]
     _, _, rep_h = ctx.hooi_dense(X, (6, 6, 6), init="hosvd", max_sweeps=60, tol=1e-12)
     assert abs(rep["residual"] - rep_h["residual"]) < 1e-9
+
+
+@pytest.mark.gpu
+def test_training_adds_over_an_untrained_decoder(ctx, small_model):
+    """Ablation on held-out tensors: the same sketch-and-refine pipeline with
+    an untrained (random orthonormal) decoder starts from a much worse fit and
+    needs no fewer sweeps than the trained one; a fixed Chebyshev basis (the
+    family's own generating polynomials, no training) is reported beside it."""
+    from diana_tucker_b200 import warmstart
+    models = {k: warmstart.ablation_model(small_model, k) for k in ("random", "chebyshev")}
+    rows = warmstart.evaluate(ctx, range(2000, 2006), small_model, models=models)
+    s = warmstart.summarize(rows)
+    rnd, cheb = s["ablation"]["random"], s["ablation"]["chebyshev"]
+    assert s["mean_fit_init_warm"] > rnd["mean_fit_init"] + 0.05
+    assert s["mean_sweeps_warm"] <= rnd["mean_sweeps"]
+    assert s["mean_sweeps_warm_strict"] <= rnd["mean_sweeps_strict"]
+    assert cheb["mean_fit_init"] is not None and s["mean_sweeps_warm"] is not None
