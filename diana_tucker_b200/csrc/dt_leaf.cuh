@@ -28,6 +28,12 @@ bool subspace_small_supported(int64_t n, int64_t R);
 void subspace_small(dt_ctx *ctx, const double *S, int64_t n, double *L, int64_t R, int iters,
                     int *flag, double *g2_out);
 
+// T (R0 x R1 x S col-major, FP64) = X x_0 U0^T x_1 U1^T for the FP32 X seen
+// as I0 x I1 x S, in one pass over X on the FP64 tensor cores (dt_core_proj.cu).
+bool core_slices_supported(int64_t I0, int64_t I1, int64_t R0, int64_t R1);
+void core_slices_f64(dt_ctx *ctx, const float *X, int64_t I0, int64_t I1, int64_t S,
+                     const double *U0, int64_t R0, const double *U1, int64_t R1, double *T);
+
 // out[0] = trace(U^T S U) for S n x n, U n x R (FP64).
 void quad_trace(dt_ctx *ctx, const double *S, int64_t n, const double *U, int64_t R, double *out);
 
