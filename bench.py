@@ -447,7 +447,10 @@ def run_ours(args):
         out["clocks"] = clk
     if args.ttmc and world == 1:
         _log("sparse TTMc")
-        out["ttmc"] = _ttmc(ctx, peak, args.ttmc_draws)
+        out["ttmc"] = _ttmc(ctx, peak, args.ttmc_draws, args.cpu and rank == 0)
+    if args.cfg1 and world == 1:
+        _log("200^3 FP64 HOOI")
+        out["dense_200cube"] = _cfg1(ctx, args.steps, args.cpu and rank == 0)
     if args.batched and world == 1:
         _log("batched HOOI (4096 small tensors)")
         out["batched"] = _batched(ctx, args.steps, args.cpu and rank == 0)
@@ -466,10 +469,14 @@ def run_ours(args):
         print(json.dumps(out), flush=True)
 
 
-def _ttmc(ctx, peak, draws=50_000_000):
+def _ttmc(ctx, peak, draws=50_000_000, cpu=False):
     """Sparse TTMc bandwidth on the 2,000,000 x 200,000 x 50,000 COO tensor
     (50M Zipf(1.1) draws, merged; fewer with --ttmc-draws), ranks 16^3: one
-    sparse HOOI sweep with the TTMc launches timed by CUDA events."""
+    sparse HOOI sweep with the TTMc launches timed by CUDA events; then the
+    configured sparse HOOI (random orthonormal init, 10 sweeps) timed whole,
+    and, with cpu, one sweep of the C restatement of the reference's sparse
+    HOOI (OpenMP, all host threads) from the same start, checked against the
+    GPU's one-sweep residual."""
     from diana_tucker_b200 import datasets
     t0 = time.time()
     if draws == 50_000_000:
@@ -500,7 +507,27 @@ def _ttmc(ctx, peak, draws=50_000_000):
     # of that traffic is nnz * 128 B per mode.
     gather = float(len(vals)) * 3 * (16 * 8)
     eff = (rep["ttm_x_bytes"] + gather) / (rep["ttm_x_ms"] * 1e-3) / 1e9 if rep["ttm_x_ms"] else 0.0
+    # The configured run: 10 sweeps from the same random orthonormal start.
+    sp.hooi(R, 10, Ut)
+    _, _, rep10 = sp.hooi(R, 10, Ut)
+    hooi10 = {"ms": round(rep10["device_ms"], 3), "sweeps": 10,
+              "ms_per_sweep": round(rep10["device_ms"] / 10, 3),
+              "rel_err": rep10["residual"],
+              "workload": "sparse HOOI ranks 16^3, random orthonormal init (seed 2), 10 sweeps"}
     sp.close()
+    if cpu:
+        from oracle import sparse as osp
+        t1 = time.perf_counter()
+        _, _, res_cpu = osp.hooi(idx, vals, shape, R, 1, Ut)
+        cpu_ms = (time.perf_counter() - t1) * 1e3
+        hooi10["cpu_baseline"] = {
+            "value": round(cpu_ms, 1), "unit": "ms per sweep", "kind": "port",
+            "cores": os.cpu_count(), "cpu_model": _cpu_model(),
+            "sample": "one sweep of the C restatement of the reference's sparse HOOI "
+                      "(sp_hooi_als.tpp:67-118; OpenMP over rows) on the whole tensor from the "
+                      "same start; the GPU figure to compare is ms_per_sweep",
+            "rel_err_1_sweep": res_cpu, "gpu_rel_err_1_sweep": rep["residual"],
+            "rel_err_gap_1_sweep": abs(res_cpu - rep["residual"])}
     return {"value": round(gbs, 1), "unit": "GB/s", "frac_of_hbm": round(gbs / peak, 4),
             "bytes_def": "fibre layout read (12 B/nonzero + 8 B/fibre slot) + Y rows written "
                          "+ factors",
@@ -509,7 +536,68 @@ def _ttmc(ctx, peak, draws=50_000_000):
             "coo_bytes": coo, "coo_gbs": round(coo_gbs, 1),
             "coo_frac_of_hbm": round(coo_gbs / peak, 4),
             "gather_bytes_lower_bound": gather, "with_gathers_gbs": round(eff, 1),
-            "sweep_ms": rep["device_ms"], "gen_s": round(gen_s, 1)}
+            "sweep_ms": rep["device_ms"], "gen_s": round(gen_s, 1), "hooi": hooi10}
+
+
+def _cfg1(ctx, steps, cpu):
+    """The 200x200x200 FP64 Tucker tensor (core 10^3, noise N(0,1e-4), seed 0):
+    plain FP64 HOOI, ranks (10,10,10), HOSVD init, <= 25 sweeps or a residual
+    change < 1e-8 -- on the GPU (device events, X resident; and end to end from
+    host memory) and, with cpu, the reference's own HOOI sweep (Function::ttm +
+    ALS_ with the same HOSVD init and stop rule, compiled from its sources,
+    all host threads)."""
+    import numpy as np
+    import torch
+
+    from diana_tucker_b200 import DT_PREC_FP64, datasets
+    X = datasets.dense_200cube_fp64()
+    flat = np.ascontiguousarray(X.reshape(-1, order="F"))
+    Xd = torch.from_numpy(flat).to(f"cuda:{ctx.device}")
+    kw = dict(init="hosvd", max_sweeps=25, tol=1e-8, precision=DT_PREC_FP64, shape=X.shape)
+    for _ in range(3):
+        ctx.hooi_dense(Xd, (10, 10, 10), device_out=True, **kw)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n = max(3, steps)
+    e0.record()
+    for _ in range(n):
+        _, _, rep = ctx.hooi_dense(Xd, (10, 10, 10), device_out=True, **kw)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / n
+    Xh = torch.from_numpy(flat).pin_memory()
+    t = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        ctx.hooi_dense(Xh, (10, 10, 10), **kw)
+        t.append((time.perf_counter() - t0) * 1e3)
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "large_oracle.json")) as f:
+            oref = json.load(f)["dense_200cube_r10"]["residual"]
+    except Exception:
+        oref = None
+    out = {"ms": round(ms, 3), "e2e_ms": round(float(np.median(t)), 3), "sweeps": rep["sweeps"],
+           "rel_err": rep["residual"], "rel_err_oracle": oref,
+           "rel_err_gap": abs(rep["residual"] - oref) if oref is not None else None,
+           "h2d_bytes": int(flat.nbytes),
+           "workload": "200^3 FP64 Tucker(10^3) + N(0,1e-4), seed 0; FP64 HOOI ranks 10^3, "
+                       "HOSVD init, <= 25 sweeps or residual change < 1e-8"}
+    if cpu:
+        from oracle import ref
+        if ref.available():
+            ref.hooi_harness(X, (10, 10, 10), 25, 1e-8)
+            t0 = time.perf_counter()
+            _, _, hist = ref.hooi_harness(X, (10, 10, 10), 25, 1e-8)
+            cms = (time.perf_counter() - t0) * 1e3
+            out["cpu_baseline"] = {
+                "value": round(cms, 1), "unit": "ms", "kind": "reference",
+                "cores": os.cpu_count(), "cpu_model": _cpu_model(), "rel_err": hist[-1],
+                "sweeps": len(hist),
+                "sample": "the whole decomposition: the reference's Function::gram + dsyevd "
+                          "HOSVD init and its Function::ttm + ALS_ sweeps (hooi_als.tpp:94-114) "
+                          "to the same stop rule, FP64, all OpenMP/OpenBLAS threads"}
+    del Xd
+    return out
 
 
 def _ref_batched_worker(args):
@@ -711,6 +799,7 @@ def main(argv=None):
     ap.add_argument("--no-cpu", dest="cpu", action="store_false")
     ap.add_argument("--no-warmstart", dest="warmstart", action="store_false")
     ap.add_argument("--no-batched", dest="batched", action="store_false")
+    ap.add_argument("--no-cfg1", dest="cfg1", action="store_false")
     ap.add_argument("--ttmc-draws", type=int, default=50_000_000,
                     help="Zipf draws of the sparse tensor (50M is the configured workload)")
     ap.add_argument("--ws-train", type=int, default=1500,
