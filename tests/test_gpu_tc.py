@@ -103,7 +103,7 @@ def test_mixed_hooi_falls_back_to_fp64_outside_layout_rules(ctx):
 
 
 @pytest.mark.parametrize("shape,ranks", [((96, 80, 72, 64), (16, 12, 8, 16)),
-                                         ((64, 48, 40), (8, 6, 5))])
+                                         ((64, 48, 40), (8, 8, 8))])
 def test_pair_node_leaf_grams_match_formed_unfoldings(shape, ranks, monkeypatch):
     """The pair nodes' leaf Grams taken straight from the pair tensor give the
     same decomposition as forming every Y_(n) and its Gram (both against the
