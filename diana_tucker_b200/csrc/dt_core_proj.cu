@@ -27,6 +27,7 @@ namespace dt {
 namespace {
 
 constexpr int CP_THREADS = 256;
+constexpr int CP_MAXT = 16;  // W tiles per warp: (RM / 8) x ceil(I1 / 8) / 8
 
 __device__ __forceinline__ void cpa16(void *smem, const void *gmem) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
@@ -46,7 +47,7 @@ __device__ __forceinline__ void cpa_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                  : "+d"(d0), "+d"(d1)
                  : "d"(a), "d"(b));
 }
@@ -119,26 +120,53 @@ __global__ void __launch_bounds__(CP_THREADS, 1) core_slices_kernel(const CoreSl
         }
         __syncthreads();
         const float *Xc = Xs + st * stage_floats;
-        // W = U0^T X_s: tiles (mt over r0, nt over i1), k over i0.
-        for (int tile = w; tile < mt_w * nt_w; tile += CP_THREADS / 32) {
-            const int mt = tile % mt_w, nt = tile / mt_w;
-            const double *arow = U0t + (8 * mt + g) * a.up + t;
-            const int col = min(8 * nt + g, a.I1 - 1);  // columns past I1 are discarded
-            const float *bcol = Xc + col * a.xp + t;
-            double d0 = 0.0, d1 = 0.0;
-            for (int k = 0; k < a.k0; k += 4) dmma(d0, d1, arow[k], (double)bcol[k]);
-            const int c0 = 8 * nt + 2 * t;
-            if (c0 < a.I1) W[(8 * mt + g) * a.up + c0] = d0;
-            if (c0 + 1 < a.I1) W[(8 * mt + g) * a.up + c0 + 1] = d1;
+        // W = U0^T X_s: tiles (mt over r0, nt over i1), k over i0.  Warp w
+        // owns tiles w, w + 8, ...; their k-loops run interleaved.
+        {
+            const double *arow[CP_MAXT];
+            const float *bcol[CP_MAXT];
+            double d0[CP_MAXT], d1[CP_MAXT];
+            int ntl = 0;
+#pragma unroll
+            for (int q = 0; q < CP_MAXT; q++) {
+                const int tile = w + 8 * q;
+                const bool on = tile < mt_w * nt_w;
+                const int mt = on ? tile % mt_w : 0, nt = on ? tile / mt_w : 0;
+                arow[q] = U0t + (8 * mt + g) * a.up + t;
+                bcol[q] = Xc + min(8 * nt + g, a.I1 - 1) * a.xp + t;  // columns past I1 discarded
+                d0[q] = d1[q] = 0.0;
+                ntl += on;
+            }
+            for (int k = 0; k < a.k0; k += 4) {
+#pragma unroll
+                for (int q = 0; q < CP_MAXT; q++)
+                    if (q < ntl) dmma(d0[q], d1[q], arow[q][k], (double)bcol[q][k]);
+            }
+#pragma unroll
+            for (int q = 0; q < CP_MAXT; q++) {
+                if (q >= ntl) break;
+                const int tile = w + 8 * q, mt = tile % mt_w, nt = tile / mt_w;
+                const int c0 = 8 * nt + 2 * t;
+                if (c0 < a.I1) W[(8 * mt + g) * a.up + c0] = d0[q];
+                if (c0 + 1 < a.I1) W[(8 * mt + g) * a.up + c0 + 1] = d1[q];
+            }
         }
         __syncthreads();
-        // T_s = W U1: tiles (mt over r0, nt over r1), k over i1.
+        // T_s = W U1: tiles (mt over r0, nt over r1), k over i1, two
+        // accumulator pairs per tile (even / odd k-steps).
         for (int tile = w; tile < mt_w * mt_w; tile += CP_THREADS / 32) {
             const int mt = tile % mt_w, nt = tile / mt_w;
             const double *arow = W + (8 * mt + g) * a.up + t;
             const double *brow = U1t + (8 * nt + g) * a.up + t;
-            double d0 = 0.0, d1 = 0.0;
-            for (int k = 0; k < a.k1; k += 4) dmma(d0, d1, arow[k], brow[k]);
+            double d0 = 0.0, d1 = 0.0, e0 = 0.0, e1 = 0.0;
+            int k = 0;
+            for (; k + 8 <= a.k1; k += 8) {
+                dmma(d0, d1, arow[k], brow[k]);
+                dmma(e0, e1, arow[k + 4], brow[k + 4]);
+            }
+            for (; k < a.k1; k += 4) dmma(d0, d1, arow[k], brow[k]);
+            d0 += e0;
+            d1 += e1;
             const int r0 = 8 * mt + g, r1 = 8 * nt + 2 * t;
             double *out = a.T + s * a.R0 * a.R1;
             if (r0 < a.R0) {
@@ -166,6 +194,8 @@ bool core_slices_supported(int64_t I0, int64_t I1, int64_t R0, int64_t R1) {
     if (I0 < 1 || I1 < 1 || R0 < 1 || R1 < 1 || R0 > 32 || R1 > 32 || R0 > I0 || R1 > I1)
         return false;
     const int RM = (int)std::max<int64_t>(8, ((std::max(R0, R1) + 7) / 8) * 8);
+    // W tiles per warp within CP_MAXT.
+    if ((RM / 8) * ((I1 + 7) / 8) > 8 * CP_MAXT) return false;
     return I0 <= 1024 && I1 <= 1024 && core_slices_smem(I0, I1, RM) <= 200 * 1024;
 }
 

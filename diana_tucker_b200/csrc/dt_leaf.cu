@@ -38,49 +38,79 @@ struct SliceView {
     int nc;
 };
 
+constexpr int SG_MAXCG = 64;  // slices per CTA at most
+
 template <int BS>
-__global__ void __launch_bounds__(SG_THREADS) slice_gram_kernel(SliceView v, int side, int cg,
+__global__ void __launch_bounds__(SG_THREADS, 2) slice_gram_kernel(SliceView v, int side, int cg,
                                                                  const double *__restrict__ U,
                                                                  int R, double *__restrict__ part) {
     // side 0: S over mode p, W = T_c U_q (contract mode q); side 1: the reverse.
     extern __shared__ float sgm[];
+    __shared__ int64_t coff[SG_MAXCG];
     const int na = side == 0 ? v.np : v.nq;  // S dimension
     const int nb = side == 0 ? v.nq : v.np;  // contracted dimension
     const int pitch = v.np + 1;              // slice stored [j][i] with padded rows
     const int RP = (R + 3) & ~3;
+    const int WP = RP + 1;                   // odd pitch: the S-phase loads spread over banks
     float *Zs = sgm;                              // cg x nq x pitch
     float *Us = Zs + (size_t)cg * v.nq * pitch;   // nb x RP
-    float *Ws = Us + (size_t)nb * RP;             // na x RP (row a at a * RP)
+    float *Ws = Us + (size_t)nb * RP;             // na x WP (row a at a * WP)
     const int c0 = blockIdx.x * cg;
     const int ncg = min(cg, v.nc - c0);
     pdl_trigger();
+    if (threadIdx.x < ncg) {
+        const int64_t c = c0 + threadIdx.x;
+        coff[threadIdx.x] = (c % v.clo) + (c / v.clo) * v.chs;
+    }
     pdl_wait();
     for (int e = threadIdx.x; e < nb * RP; e += SG_THREADS) {
         const int b = e / RP, r = e - b * RP;
         Us[e] = r < R ? (float)U[b + (int64_t)nb * r] : 0.f;
     }
-    // Load the CTA's slices.  When the low part of c is the contiguous index
-    // (clo > 1), consecutive threads take consecutive c.
-    const int64_t total = (int64_t)ncg * v.np * v.nq;
-    const bool c_inner = v.clo > 1;
-    for (int64_t e = threadIdx.x; e < total; e += SG_THREADS) {
-        int cc, i, j;
-        if (c_inner) {
-            cc = (int)(e % ncg);
-            const int64_t r = e / ncg;
-            i = (int)(r % v.np);
-            j = (int)(r / v.np);
-        } else {
-            i = (int)(e % v.np);
-            const int64_t r = e / v.np;
-            j = (int)(r % v.nq);
-            cc = (int)(r / v.nq);
+    __syncthreads();
+    // Load the CTA's slices.  The element index runs over three digits (the
+    // contiguous one fastest: c when the low part of c is contiguous in T,
+    // clo > 1; else i); each thread steps by SG_THREADS with carries, so the
+    // loop divides nothing.
+    {
+        const bool c_inner = v.clo > 1;
+        const int n0 = c_inner ? ncg : v.np, n1 = c_inner ? v.np : v.nq;
+        const int total = ncg * v.np * v.nq;
+        const int k0 = SG_THREADS % n0, k1 = (SG_THREADS / n0) % n1,
+                  k2 = SG_THREADS / (n0 * n1);
+        int d0 = threadIdx.x % n0, d1 = (threadIdx.x / n0) % n1, d2 = threadIdx.x / (n0 * n1);
+        constexpr int UNR = 4;  // elements per thread and round: 2 UNR loads in flight
+        for (int e = threadIdx.x; e < total; e += UNR * SG_THREADS) {
+            int64_t off[UNR];
+            int dst[UNR];
+#pragma unroll
+            for (int u = 0; u < UNR; u++) {
+                const int cc = c_inner ? d0 : d2, i = c_inner ? d1 : d0, j = c_inner ? d2 : d1;
+                const bool on = e + u * SG_THREADS < total;
+                off[u] = on ? i * v.sp + j * v.sq + coff[cc] : 0;
+                dst[u] = on ? (cc * v.nq + j) * pitch + i : -1;
+                d0 += k0;
+                d1 += k1;
+                d2 += k2;
+                if (d0 >= n0) {
+                    d0 -= n0;
+                    d1++;
+                }
+                if (d1 >= n1) {
+                    d1 -= n1;
+                    d2++;
+                }
+            }
+            float hv[UNR], lv[UNR];
+#pragma unroll
+            for (int u = 0; u < UNR; u++) {
+                hv[u] = dst[u] >= 0 ? __bfloat162float(v.hi[off[u]]) : 0.f;
+                lv[u] = dst[u] >= 0 && v.lo ? __bfloat162float(v.lo[off[u]]) : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < UNR; u++)
+                if (dst[u] >= 0) Zs[dst[u]] = hv[u] + lv[u];
         }
-        const int64_t c = c0 + cc;
-        const int64_t off = i * v.sp + j * v.sq + (c % v.clo) + (c / v.clo) * v.chs;
-        float x = __bfloat162float(v.hi[off]);
-        if (v.lo) x += __bfloat162float(v.lo[off]);
-        Zs[((size_t)cc * v.nq + j) * pitch + i] = x;
     }
     __syncthreads();
     // This thread's BS x BS block of S: rows bi*BS.., columns bj*BS.. of the
@@ -111,7 +141,7 @@ __global__ void __launch_bounds__(SG_THREADS) slice_gram_kernel(SliceView v, int
                 }
                 if (b < nb) s0 = fmaf(Z[a * pitch + b], Us[b * RP + r], s0);
             }
-            Ws[a * RP + r] = s0 + s1;
+            Ws[a * WP + r] = s0 + s1;
         }
         __syncthreads();
         for (int r = 0; r < R; r++) {
@@ -119,8 +149,8 @@ __global__ void __launch_bounds__(SG_THREADS) slice_gram_kernel(SliceView v, int
 #pragma unroll
             for (int x = 0; x < BS; x++) {
                 const int ia = bi * BS + x, ib = bj * BS + x;
-                wa[x] = ia < na ? (double)Ws[ia * RP + r] : 0.0;
-                wb[x] = ib < na ? (double)Ws[ib * RP + r] : 0.0;
+                wa[x] = ia < na ? (double)Ws[ia * WP + r] : 0.0;
+                wb[x] = ib < na ? (double)Ws[ib * WP + r] : 0.0;
             }
 #pragma unroll
             for (int x = 0; x < BS; x++)
@@ -146,8 +176,17 @@ __global__ void sum_parts_fixed_kernel(const double *__restrict__ part, int nz, 
     pdl_wait();
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
          e += (int64_t)gridDim.x * blockDim.x) {
+        // Eight loads in flight, added in z order.
         double s = 0.0;
-        for (int z = 0; z < nz; z++) s += part[(int64_t)z * n + e];
+        int z = 0;
+        for (; z + 8 <= nz; z += 8) {
+            double v[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) v[q] = part[(int64_t)(z + q) * n + e];
+#pragma unroll
+            for (int q = 0; q < 8; q++) s += v[q];
+        }
+        for (; z < nz; z++) s += part[(int64_t)z * n + e];
         S[e] = s;
     }
 }
@@ -202,30 +241,51 @@ __global__ void __launch_bounds__(256) quad_trace_kernel(const double *__restric
 //  * With g2_out, the final trace(Q^T S Q) (the norm^2 of the core of the
 //    last mode, used for the sweep residual) is written there.
 // ---------------------------------------------------------------------------
+// A pure function of its operands (no volatile): the compiler may hoist the
+// shared-memory loads of later k-steps ahead of earlier MMAs.
 __device__ __forceinline__ void dmma884(double &d0, double &d1, double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
-                 : "+d"(d0), "+d"(d1)
-                 : "d"(a), "d"(b));
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+        : "+d"(d0), "+d"(d1)
+        : "d"(a), "d"(b));
 }
 
 __host__ __device__ constexpr int pitch4(int n) { return n + ((4 - n % 16) + 16) % 16; }
 
 constexpr int SS_THREADS = 256;
+constexpr int SS_MAXT = 8;  // output tiles per warp of one product (npad <= 128, RM <= 32)
 
 // Z (npad x RM, pitch pz) = S (npad x npad, pitch ps) A (npad x RM, pitch pa).
+// Warp w owns tiles w, w + 8, ...; their k-loops run interleaved (independent
+// accumulators), so the MMA latency overlaps across tiles.
 template <int RM>
 __device__ void ss_product(const double *S, int ps, const double *A, int pa, double *Z, int pz,
                            int npad) {
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     const int mt_n = npad / 8, tiles = mt_n * (RM / 8);
-    for (int tile = w; tile < tiles; tile += SS_THREADS / 32) {
-        const int mt = tile % mt_n, nt = tile / mt_n;
-        double d0 = 0.0, d1 = 0.0;
-        const double *sa = S + 8 * mt + g + (int64_t)ps * t;
-        const double *sb = A + t + (int64_t)pa * (8 * nt + g);
-        for (int k = 0; k < npad; k += 4) dmma884(d0, d1, sa[(int64_t)ps * k], sb[k]);
-        Z[8 * mt + g + (int64_t)pz * (8 * nt + 2 * t)] = d0;
-        Z[8 * mt + g + (int64_t)pz * (8 * nt + 2 * t + 1)] = d1;
+    const double *sa[SS_MAXT], *sb[SS_MAXT];
+    double d0[SS_MAXT], d1[SS_MAXT];
+    int nt = 0;
+#pragma unroll
+    for (int q = 0; q < SS_MAXT; q++) {
+        const int tile = w + 8 * q;
+        const bool on = tile < tiles;
+        const int mt = on ? tile % mt_n : 0, ntl = on ? tile / mt_n : 0;
+        sa[q] = S + 8 * mt + g + (int64_t)ps * t;
+        sb[q] = A + t + (int64_t)pa * (8 * ntl + g);
+        d0[q] = d1[q] = 0.0;
+        nt += on;
+    }
+    for (int k = 0; k < npad; k += 4) {
+#pragma unroll
+        for (int q = 0; q < SS_MAXT; q++)
+            if (q < nt) dmma884(d0[q], d1[q], sa[q][(int64_t)ps * k], sb[q][k]);
+    }
+#pragma unroll
+    for (int q = 0; q < SS_MAXT; q++) {
+        if (q >= nt) break;
+        const int tile = w + 8 * q, mt = tile % mt_n, ntl = tile / mt_n;
+        Z[8 * mt + g + (int64_t)pz * (8 * ntl + 2 * t)] = d0[q];
+        Z[8 * mt + g + (int64_t)pz * (8 * ntl + 2 * t + 1)] = d1[q];
     }
 }
 
@@ -235,18 +295,26 @@ template <int RM>
 __device__ bool ss_cholqr(double *Z, int pz, int n, int npad, int R, double *Gs, int *bad) {
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     constexpr int NT = RM / 8;
+    double *Dinv = Gs + RM * RM;  // 1 / R(k, k)
     for (int tile = w; tile < NT * NT; tile += SS_THREADS / 32) {
         const int ma = tile % NT, mb = tile / NT;
-        double d0 = 0.0, d1 = 0.0;
+        // Two accumulator pairs (even / odd k-steps), added at the end.
+        double d0 = 0.0, d1 = 0.0, e0 = 0.0, e1 = 0.0;
         const double *za = Z + t + (int64_t)pz * (8 * ma + g);
         const double *zb = Z + t + (int64_t)pz * (8 * mb + g);
-        for (int k = 0; k < npad; k += 4) dmma884(d0, d1, za[k], zb[k]);
-        Gs[(8 * ma + g) * RM + 8 * mb + 2 * t] = d0;
-        Gs[(8 * ma + g) * RM + 8 * mb + 2 * t + 1] = d1;
+        int k = 0;
+        for (; k + 8 <= npad; k += 8) {
+            dmma884(d0, d1, za[k], zb[k]);
+            dmma884(e0, e1, za[k + 4], zb[k + 4]);
+        }
+        for (; k < npad; k += 4) dmma884(d0, d1, za[k], zb[k]);
+        Gs[(8 * ma + g) * RM + 8 * mb + 2 * t] = d0 + e0;
+        Gs[(8 * ma + g) * RM + 8 * mb + 2 * t + 1] = d1 + e1;
     }
     __syncthreads();
     if (w == 0) {
         // Lane j holds column j of the Gram; on exit column j of R (upper).
+        // One reciprocal square root per pivot, no division.
         double c[RM];
 #pragma unroll
         for (int i = 0; i < RM; i++) c[i] = (lane < R && i < R) ? Gs[i * RM + lane] : 0.0;
@@ -257,9 +325,9 @@ __device__ bool ss_cholqr(double *Z, int pz, int n, int npad, int R, double *Gs,
             if (k >= R) break;
             const double dkk = __shfl_sync(0xffffffffu, c[k], k);
             if (!(dkk > 1e-28 * g00)) ok = false;
-            const double rkk = sqrt(fmax(dkk, 1e-300));
-            const double inv = 1.0 / rkk;
-            c[k] = lane == k ? rkk : (lane > k ? c[k] * inv : c[k]);
+            const double inv = rsqrt(fmax(dkk, 1e-300));
+            if (lane == k) Dinv[k] = inv;
+            c[k] = lane == k ? dkk * inv : (lane > k ? c[k] * inv : c[k]);
 #pragma unroll
             for (int i = k + 1; i < RM; i++) {
                 if (i >= R) break;
@@ -276,7 +344,8 @@ __device__ bool ss_cholqr(double *Z, int pz, int n, int npad, int R, double *Gs,
     }
     __syncthreads();
     if (*bad) return false;
-    // Row i: q_c = (z_c - sum_{k<c} q_k R(k, c)) / R(c, c).
+    // Row i: q_c = (z_c - sum_{k<c} q_k R(k, c)) / R(c, c); the updates of the
+    // later columns are independent of each other.
     for (int i = threadIdx.x; i < n; i += SS_THREADS) {
         double z[RM];
 #pragma unroll
@@ -284,7 +353,7 @@ __device__ bool ss_cholqr(double *Z, int pz, int n, int npad, int R, double *Gs,
 #pragma unroll
         for (int k = 0; k < RM; k++) {
             if (k >= R) break;
-            const double q = z[k] / Gs[k * RM + k];
+            const double q = z[k] * Dinv[k];
             z[k] = q;
 #pragma unroll
             for (int c = k + 1; c < RM; c++)
@@ -412,7 +481,8 @@ void subspace_small(dt_ctx *ctx, const double *S, int64_t n, double *L, int64_t 
     const int npad = (int)((n + 7) & ~int64_t(7));
     const int p = pitch4(npad);
     auto go = [&](auto kernel, int RM) {
-        const size_t smem = ((size_t)p * npad + 2 * (size_t)p * RM + (size_t)RM * RM) * sizeof(double);
+        const size_t smem =
+            ((size_t)p * npad + 2 * (size_t)p * RM + (size_t)RM * RM + RM) * sizeof(double);
         smem_limit(ctx, kernel, smem);
         DT_LAUNCH_PDL(ctx, kernel, 1, SS_THREADS, smem, S, (int)n, L, (int)R, iters, flag, g2_out);
     };
@@ -431,7 +501,8 @@ bool pair_gram_supported(int64_t np, int64_t nq, int64_t R) {
 
 size_t pair_gram_scratch_doubles(int64_t np, int64_t nq, int64_t nc) {
     const int64_t n = std::max(np, nq);
-    return (size_t)std::min<int64_t>(nc, 256) * n * n;
+    const int64_t nz = std::max<int64_t>(std::min<int64_t>(nc, 256), (nc + SG_MAXCG - 1) / SG_MAXCG);
+    return (size_t)nz * n * n;
 }
 
 void pair_gram(dt_ctx *ctx, const __nv_bfloat16 *Th, const __nv_bfloat16 *Tl, int64_t np,
@@ -445,14 +516,18 @@ void pair_gram(dt_ctx *ctx, const __nv_bfloat16 *Th, const __nv_bfloat16 *Tl, in
     // Slices per CTA: as many CTAs as SMs where the slices allow, the
     // group's slices staged together within ~160 KB of shared memory.
     const size_t slice_bytes = (size_t)nq * (np + 1) * sizeof(float);
-    const size_t fixed = ((size_t)nb * RP + (size_t)na * RP) * sizeof(float);
-    int cg = (int)std::max<int64_t>(1, (nc + ctx->num_sms - 1) / ctx->num_sms);
+    const size_t fixed = ((size_t)nb * RP + (size_t)na * (RP + 1)) * sizeof(float);
+    // Slices per CTA: one while the slices fill two CTAs per SM, more only
+    // for a long slice list.
+    int cg = (int)std::max<int64_t>(1, (nc + 2 * ctx->num_sms - 1) / (2 * ctx->num_sms));
+    cg = std::min(cg, SG_MAXCG);
     while (cg > 1 && fixed + cg * slice_bytes > 160 * 1024) cg--;
     int64_t nz = (nc + cg - 1) / cg;
-    while ((size_t)nz * na * na > part_doubles) {
+    while ((size_t)nz * na * na > part_doubles && cg < SG_MAXCG) {
         cg++;
         nz = (nc + cg - 1) / cg;
     }
+    DT_CHECK_ARG((size_t)nz * na * na <= part_doubles, "pair_gram: scratch too small");
     DT_CHECK_ARG(fixed + cg * slice_bytes <= 220 * 1024, "pair_gram: slices too large");
     const size_t smem = fixed + cg * slice_bytes;
     auto go = [&](auto kernel) {
