@@ -21,7 +21,6 @@
 #include <algorithm>
 
 #include "dt_kernels.cuh"
-#include "dt_leaf.cuh"
 
 namespace dt {
 namespace {
@@ -46,8 +45,9 @@ template <int N>
 __device__ __forceinline__ void cpa_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
+// volatile: the compiler must not execute a guarded MMA unconditionally.
 __device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
-    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                  : "+d"(d0), "+d"(d1)
                  : "d"(a), "d"(b));
 }

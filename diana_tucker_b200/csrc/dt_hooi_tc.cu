@@ -18,7 +18,6 @@
 
 #include "dt_hooi.cuh"
 #include "dt_kernels.cuh"
-#include "dt_leaf.cuh"
 #include "dt_tc_host.cuh"
 
 namespace dt {
@@ -44,11 +43,9 @@ struct MixedHooi {
     const float *X32 = nullptr;
     DevMem X32own, Xh, Xl;
     std::vector<DevMem> U;
-    DevMem S, work, flag, err, scal, Gs, lpart;
-    size_t lpart_doubles = 0;
+    DevMem S, work, flag, err, scal, Gs;
     bool split = false;   // intermediates, U and the Gram operands as hi + lo
     bool xsplit = false;  // X itself as hi + lo (else X in BF16 hi only)
-    bool pair_gram_on = true;  // pair nodes: leaf Grams straight from the pair tensor
     DenseHooi helper;  // initial factors (same generators as the FP64 driver)
     LaunchTimer *xtimer = nullptr;
     SweepGraph *g_bf16 = nullptr, *g_split = nullptr;  // captured sweeps (or null)
@@ -189,60 +186,15 @@ struct MixedHooi {
         const __nv_bfloat16 *yh = Y.hi.as<__nv_bfloat16>();
         const __nv_bfloat16 *yl = split ? Y.lo.as<__nv_bfloat16>() : nullptr;
         tc_gram(ctx, yh, yl, I[n], K, S.as<double>(), err.as<int>());
-        leaf_subspace(n, I[n], nullptr);
+        subspace_iter(ctx, S.as<double>(), I[n], U[n].as<double>(), R[n], opts.inner_iters,
+                      work.as<double>(), flag.as<int>());
         if (n == N - 1)
             core_rows(ctx, yh, yl, I[n], K, U[n].as<double>(), R[n], Gs.as<double>(),
                       scal.as<double>() + 1);
     }
 
-    // Pair node {p, p + 1} of the tree whose leaves take their Grams from the
-    // pair tensor T itself (dt_leaf.cu): T's modes p, p+1 keep I, the others
-    // are contracted to R.
-    bool pair_ok(int p, const int64_t *shape) const {
-        int64_t nc = 1;
-        for (int k = 0; k < N; k++)
-            if (k != p && k != p + 1) nc *= shape[k];
-        return pair_gram_on && nc <= (int64_t(1) << 31) &&
-               pair_gram_supported(shape[p], shape[p + 1], R[p + 1]) &&
-               pair_gram_supported(shape[p], shape[p + 1], R[p]);
-    }
-
-    void pair(int p, const __nv_bfloat16 *Th, const __nv_bfloat16 *Tl, const int64_t *shape) {
-        const int q = p + 1;
-        int64_t clo = 1, chi = 1;
-        for (int k = 0; k < p; k++) clo *= shape[k];
-        for (int k = q + 1; k < N; k++) chi *= shape[k];
-        const int64_t np = shape[p], nq = shape[q];
-        const int64_t sp = clo, sq = clo * np, chs = clo * np * nq, nc = clo * chi;
-        // Leaf p: T x_q U_q^T, then leaf q with the new U_p.  The sweep's
-        // ||G||^2 = trace(U^T S U) of the last mode.
-        pair_gram(ctx, Th, Tl, np, nq, sp, sq, clo, chs, nc, 0, U[q].as<double>(), R[q],
-                  lpart.as<double>(), lpart_doubles, S.as<double>());
-        leaf_subspace(p, np, nullptr);
-        pair_gram(ctx, Th, Tl, np, nq, sp, sq, clo, chs, nc, 1, U[p].as<double>(), R[p],
-                  lpart.as<double>(), lpart_doubles, S.as<double>());
-        leaf_subspace(q, nq, q == N - 1 ? scal.as<double>() + 1 : nullptr);
-    }
-
-    // U_n <- orth(S^inner U_n) for the Gram S of mode n (size n_n); with g2,
-    // trace(U_n^T S U_n) is written there.
-    void leaf_subspace(int n, int64_t nn, double *g2) {
-        if (subspace_small_supported(nn, R[n])) {
-            subspace_small(ctx, S.as<double>(), nn, U[n].as<double>(), R[n], opts.inner_iters,
-                           flag.as<int>(), g2);
-            return;
-        }
-        subspace_iter(ctx, S.as<double>(), nn, U[n].as<double>(), R[n], opts.inner_iters,
-                      work.as<double>(), flag.as<int>());
-        if (g2) quad_trace(ctx, S.as<double>(), nn, U[n].as<double>(), R[n], g2);
-    }
-
     void node(int lo, int hi, const __nv_bfloat16 *Th, const __nv_bfloat16 *Tl,
               const int64_t *shape) {
-        if (hi - lo == 2 && pair_ok(lo, shape)) {
-            pair(lo, Th, Tl, shape);
-            return;
-        }
         const int mid = (lo + hi + 1) / 2;  // [0,3) -> [0,2) + [2,3): long TMA rows
         for (int side = 0; side < 2; side++) {
             const int clo = side == 0 ? lo : mid, chi = side == 0 ? mid : hi;
@@ -545,20 +497,6 @@ void hooi_dense_lowprec(dt_ctx *ctx, const void *X, int dtype, int ndim, const i
         h.err.alloc(ctx, sizeof(int));
         h.scal.alloc(ctx, 4 * sizeof(double));
         h.Gs.alloc(ctx, prod(ranks, ndim) * sizeof(double));
-        // Partial Grams of the pair nodes' leaves (the largest pair of the tree).
-        {
-            // DT_DISABLE_PAIR_GRAM=1 forms every Y_(n) and its Gram instead.
-            const char *e = std::getenv("DT_DISABLE_PAIR_GRAM");
-            h.pair_gram_on = !(e && e[0] == '1');
-        }
-        for (int p = 0; p + 1 < ndim; p++) {
-            int64_t nc = 1;
-            for (int k = 0; k < ndim; k++)
-                if (k != p && k != p + 1) nc *= ranks[k];
-            h.lpart_doubles = std::max(h.lpart_doubles,
-                                       pair_gram_scratch_doubles(shape[p], shape[p + 1], nc));
-        }
-        h.lpart.alloc(ctx, h.lpart_doubles * sizeof(double));
         h.g_bf16 = &plan->g_bf16;
         h.g_split = &plan->g_split;
         ctx->hooi_plan_mixed = plan;

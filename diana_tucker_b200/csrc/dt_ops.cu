@@ -1,7 +1,6 @@
 // extern "C" operator-level entry points (the Function:: / Operator<double>
 // seam of the reference) over the FP64 kernels.
 #include "dt_kernels.cuh"
-#include "dt_leaf.cuh"
 
 using namespace dt;
 
@@ -196,12 +195,8 @@ int dt_als_f64(dt_ctx *ctx, const double *Y, int ndim, const int64_t *shape, int
         ttt_f64(ctx, y.as<double>(), y.as<double>(), v.L, v.I, v.I, v.B, S.as<double>());
         DT_CUDA(cudaMemcpyAsync(q.ptr(), l0.ptr(), v.I * R * sizeof(double),
                                 cudaMemcpyDeviceToDevice, ctx->stream));
-        if (subspace_small_supported(v.I, R))
-            subspace_small(ctx, S.as<double>(), v.I, q.as<double>(), R, iters, flag.as<int>(),
-                           nullptr);
-        else
-            subspace_iter(ctx, S.as<double>(), v.I, q.as<double>(), R, iters, work.as<double>(),
-                          flag.as<int>());
+        subspace_iter(ctx, S.as<double>(), v.I, q.as<double>(), R, iters, work.as<double>(),
+                      flag.as<int>());
         q.finish();
     });
 }

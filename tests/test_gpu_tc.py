@@ -100,28 +100,3 @@ def test_mixed_hooi_falls_back_to_fp64_outside_layout_rules(ctx):
     G, U, rep = ctx.hooi_dense(X, (3, 3, 3), init="randn", seed=1, max_sweeps=4,
                                precision=DT_PREC_BF16)
     assert rep["precision_used"] == DT_PREC_FP64
-
-
-@pytest.mark.parametrize("shape,ranks", [((96, 80, 72, 64), (16, 12, 8, 16)),
-                                         ((64, 48, 40), (8, 8, 8))])
-def test_pair_node_leaf_grams_match_formed_unfoldings(shape, ranks, monkeypatch):
-    """The pair nodes' leaf Grams taken straight from the pair tensor give the
-    same decomposition as forming every Y_(n) and its Gram (both against the
-    FP64 oracle to the method's 1e-6)."""
-    from diana_tucker_b200 import DT_PREC_BF16XH, Context, datasets
-    X = datasets.tucker_dense(shape, ranks, noise_var=1e-6, seed=12, dtype=np.float32,
-                              core_decay=0.9)
-    U0 = dense.libc_randn_init(shape, ranks, 4)
-    G2, U2, hist = dense.hooi(X.astype(np.float64), ranks, 30, U0, tol=1e-12)
-    out = {}
-    for flag in ("0", "1"):
-        monkeypatch.setenv("DT_DISABLE_PAIR_GRAM", flag)
-        with Context(0) as c:
-            G, U, rep = c.hooi_dense(X, ranks, init="randn", seed=4, max_sweeps=30, tol=1e-9,
-                                     precision=DT_PREC_BF16XH, inner_iters=2)
-        assert rep["precision_used"] == DT_PREC_BF16XH
-        assert abs(rep["residual"] - hist[-1]) < 1e-6, (flag, rep["residual"], hist[-1])
-        for n in range(len(shape)):
-            assert dense.principal_angle_max(U[n], U2[n]) < 1e-3
-        out[flag] = rep
-    assert abs(out["0"]["residual"] - out["1"]["residual"]) < 1e-6
