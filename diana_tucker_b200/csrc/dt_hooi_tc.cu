@@ -354,20 +354,6 @@ struct MixedHooi {
             std::sort(ord.begin(), ord.end(), [](int a, int b) { return a > b; });
             const void *src = X32;
             bool src_f32 = true;
-            if (N >= 3 && core_slices_supported(I[0], I[1], R[0], R[1])) {
-                // Modes 0 and 1 in one pass over X (FP64 tensor cores), the
-                // others from the small result.
-                DevMem nxt(ctx, R[0] * R[1] * (xsize / (I[0] * I[1])) * sizeof(double));
-                core_slices_f64(ctx, X32, I[0], I[1], xsize / (I[0] * I[1]), U[0].as<double>(),
-                                R[0], U[1].as<double>(), R[1], nxt.as<double>());
-                shape[0] = R[0];
-                shape[1] = R[1];
-                cur = std::move(nxt);
-                src = cur.get();
-                src_f32 = false;
-                ord.erase(std::remove_if(ord.begin(), ord.end(), [](int m) { return m < 2; }),
-                          ord.end());
-            }
             for (int m : ord) {
                 int64_t L = 1, B = 1;
                 for (int k = 0; k < m; k++) L *= shape[k];

@@ -64,12 +64,6 @@ void subspace_iter(dt_ctx *ctx, const double *S, int64_t n, double *L, int64_t r
 void lu_inverse(dt_ctx *ctx, const double *A, int64_t n, double *Ainv, double *work,
                 int *flag);
 
-// T (R0 x R1 x S col-major, FP64) = X x_0 U0^T x_1 U1^T for the FP32 X seen
-// as I0 x I1 x S, in one pass over X on the FP64 tensor cores (dt_core_proj.cu).
-bool core_slices_supported(int64_t I0, int64_t I1, int64_t R0, int64_t R1);
-void core_slices_f64(dt_ctx *ctx, const float *X, int64_t I0, int64_t I1, int64_t S,
-                     const double *U0, int64_t R0, const double *U1, int64_t R1, double *T);
-
 // Modified Gram-Schmidt over the len1 rows of a len1 x len2 col-major A.
 void orth2_rows(dt_ctx *ctx, double *A, int64_t len1, int64_t len2);
 
