@@ -114,19 +114,37 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
     // in flight from the previous kernel.
     pdl_wait();
     // B = [U_hi | U_lo]^T (split) or U_hi^T, K-major, 128B-swizzled, zero padded.
+    // Each U entry is read once (coalesced along k), eight loads in flight per
+    // thread, and written as its hi row j and, split, its lo row j + JP.
     {
         const int kmax = a.kchunks * KC_ELEMS;
-        for (int e = threadIdx.x; e < NPAD * kmax; e += blockDim.x) {
-            const int row = e / kmax, k = e - row * kmax;
-            const int j = row % JP;
-            const bool lo_part = row >= JP;
-            float v = 0.f;
-            if (j < a.J && k < a.I) v = (float)a.U[(int64_t)k + (int64_t)a.I * j];
-            __nv_bfloat16 hi, lo;
-            bf16_split(v, hi, lo);
-            const int kc = k / KC_ELEMS, kk = k - kc * KC_ELEMS;
-            uint8_t *dst = Bt + (uint32_t)kc * NPAD * 128 + sw128_kmajor_offset(row, kk);
-            *reinterpret_cast<__nv_bfloat16 *>(dst) = lo_part ? lo : hi;
+        const int total = JP * kmax;
+        constexpr int UL = 8;
+        for (int base = 0; base < total; base += UL * (int)blockDim.x) {
+            float v[UL];
+#pragma unroll
+            for (int u = 0; u < UL; u++) {
+                const int e = base + u * (int)blockDim.x + (int)threadIdx.x;
+                const int j = e / kmax, k = e - j * kmax;
+                v[u] = (e < total && j < a.J && k < a.I)
+                           ? (float)a.U[(int64_t)k + (int64_t)a.I * j]
+                           : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < UL; u++) {
+                const int e = base + u * (int)blockDim.x + (int)threadIdx.x;
+                if (e < total) {
+                    const int j = e / kmax, k = e - j * kmax;
+                    __nv_bfloat16 hi, lo;
+                    bf16_split(v[u], hi, lo);
+                    const int kc = k / KC_ELEMS, kk = k - kc * KC_ELEMS;
+                    uint8_t *chunk = Bt + (uint32_t)kc * NPAD * 128;
+                    *reinterpret_cast<__nv_bfloat16 *>(chunk + sw128_kmajor_offset(j, kk)) = hi;
+                    if (BSPLIT)
+                        *reinterpret_cast<__nv_bfloat16 *>(
+                            chunk + sw128_kmajor_offset(j + JP, kk)) = lo;
+                }
+            }
         }
     }
     fence_proxy_async_smem();
