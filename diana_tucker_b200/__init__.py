@@ -296,9 +296,10 @@ class Context:
             dev = X.device
             # Column-major buffers: allocate the reversed shape row-major and
             # permute back.
-            G = (torch.zeros(ranks[::-1], dtype=torch.float64, device=dev)
+            # Every entry is written by the library: no fill needed.
+            G = (torch.empty(ranks[::-1], dtype=torch.float64, device=dev)
                  .permute(*range(N - 1, -1, -1)) if want_core else None)
-            U = ([torch.zeros((ranks[n], shape[n]), dtype=torch.float64, device=dev).t()
+            U = ([torch.empty((ranks[n], shape[n]), dtype=torch.float64, device=dev).t()
                   for n in range(N)] if (want_factors or U0 is not None) else None)
             if U0 is not None:
                 for n in range(N):

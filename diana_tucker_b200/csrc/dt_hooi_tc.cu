@@ -375,30 +375,37 @@ struct MixedHooi {
         const double *gsrc = cur.as<double>();
         const int gslot = 2;
         DT_CUDA(cudaEventRecord(ctx->ev_stop, ctx->stream));
-        const double g2 = read_scalar(gslot);
+        // The outputs are copied before the one synchronisation that reads
+        // ||G||^2 and the kernels' error word.
+        {
+            std::vector<DevView> outs;
+            outs.reserve(N + 1);
+            if (G_user) {
+                outs.emplace_back(ctx, G_user, prod(R, N) * sizeof(double), false, true);
+                DT_CUDA(cudaMemcpyAsync(outs.back().ptr(), gsrc, prod(R, N) * sizeof(double),
+                                        cudaMemcpyDeviceToDevice, ctx->stream));
+            }
+            if (U_user) {
+                for (int m = 0; m < N; m++) {
+                    if (!U_user[m]) continue;
+                    outs.emplace_back(ctx, U_user[m], I[m] * R[m] * sizeof(double), false, true);
+                    DT_CUDA(cudaMemcpyAsync(outs.back().ptr(), U[m].get(),
+                                            I[m] * R[m] * sizeof(double),
+                                            cudaMemcpyDeviceToDevice, ctx->stream));
+                }
+            }
+            for (auto &v : outs) v.finish();
+        }
+        double g2 = 0.0;
         int herr = 0;
+        DT_CUDA(cudaMemcpyAsync(&g2, scal.as<double>() + gslot, sizeof(double),
+                                cudaMemcpyDeviceToHost, ctx->stream));
         DT_CUDA(cudaMemcpyAsync(&herr, err.get(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         DT_CUDA(cudaStreamSynchronize(ctx->stream));
         if (herr) fail(DT_ERR_CUDA, fmt("tensor-core kernel reported error %d (wait timed out)", herr));
         float ms = 0.f;
         DT_CUDA(cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop));
         if (!std::isfinite(g2)) fail(DT_ERR_NUMERIC, "HOOI produced a non-finite core");
-        if (G_user) {
-            DevView g(ctx, G_user, prod(R, N) * sizeof(double), false, true);
-            DT_CUDA(cudaMemcpyAsync(g.ptr(), gsrc, prod(R, N) * sizeof(double),
-                                    cudaMemcpyDeviceToDevice, ctx->stream));
-            g.finish();
-        }
-        if (U_user) {
-            for (int m = 0; m < N; m++) {
-                if (!U_user[m]) continue;
-                DevView u(ctx, U_user[m], I[m] * R[m] * sizeof(double), false, true);
-                DT_CUDA(cudaMemcpyAsync(u.ptr(), U[m].get(), I[m] * R[m] * sizeof(double),
-                                        cudaMemcpyDeviceToDevice, ctx->stream));
-                u.finish();
-            }
-        }
-        DT_CUDA(cudaStreamSynchronize(ctx->stream));
         if (rep) {
             rep->sweeps = sweeps;
             rep->x_norm = std::sqrt(x2);
