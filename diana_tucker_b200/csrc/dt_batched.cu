@@ -304,6 +304,7 @@ __device__ void hooi_one(const BatchArgs &a, int t, double *sm, double *T, const
         // T = X x_3 U_3^T  (I0 x I1 x R2)
         for (int p = g.lt; p < I01; p += g.gs) {
             double acc[BMAX_R] = {};
+#pragma unroll 4
             for (int i2 = 0; i2 < I2; i2++) {
                 const double x = X[p + (int64_t)I01 * i2];
 #pragma unroll
@@ -319,6 +320,7 @@ __device__ void hooi_one(const BatchArgs &a, int t, double *sm, double *T, const
         for (int q = g.lt; q < I0 * R2; q += g.gs) {
             const int i0 = q % I0, r2 = q / I0;
             double acc[BMAX_R] = {};
+#pragma unroll 4
             for (int i1 = 0; i1 < I1; i1++) {
                 const double v = T[i0 + I0 * i1 + I01 * r2];
 #pragma unroll
@@ -336,6 +338,7 @@ __device__ void hooi_one(const BatchArgs &a, int t, double *sm, double *T, const
         for (int q = g.lt; q < I1 * R2; q += g.gs) {
             const int i1 = q % I1, r2 = q / I1;
             double acc[BMAX_R] = {};
+#pragma unroll 4
             for (int i0 = 0; i0 < I0; i0++) {
                 const double v = T[i0 + I0 * i1 + I01 * r2];
 #pragma unroll
@@ -354,6 +357,7 @@ __device__ void hooi_one(const BatchArgs &a, int t, double *sm, double *T, const
         for (int q = g.lt; q < I1 * I2; q += g.gs) {
             const int64_t base = (int64_t)I0 * q;
             double acc[BMAX_R] = {};
+#pragma unroll 4
             for (int i0 = 0; i0 < I0; i0++) {
                 const double x = X[base + i0];
 #pragma unroll
@@ -369,6 +373,7 @@ __device__ void hooi_one(const BatchArgs &a, int t, double *sm, double *T, const
         for (int q = g.lt; q < R0 * I2; q += g.gs) {
             const int r0 = q % R0, i2 = q / R0;
             double acc[BMAX_R] = {};
+#pragma unroll 4
             for (int i1 = 0; i1 < I1; i1++) {
                 const double v = T[r0 + R0 * i1 + R0I1 * i2];
 #pragma unroll

@@ -627,7 +627,7 @@ void tc_ttm(dt_ctx *ctx, const __nv_bfloat16 *Xh, const __nv_bfloat16 *Xl, int64
     const uint32_t stage_bytes = a_one * (a.split ? 2 : 1);
     const uint32_t b_bytes = ((uint32_t)a.kchunks * a.Npad * 128 + 1023) & ~1023u;
     const size_t budget = 220 * 1024;
-    int S = (int)std::min<size_t>(4, (budget - b_bytes - 1024 - 256) / stage_bytes);
+    int S = (int)std::min<size_t>(6, (budget - b_bytes - 1024 - 256) / stage_bytes);
     DT_CHECK_ARG(S >= 2, "tc_ttm: contraction length %lld too large for shared memory", (long long)I);
     a.stages = S;
     // Bytes the TMA delivers per stage (boxes are counted whole, OOB included).
