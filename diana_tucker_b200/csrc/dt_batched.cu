@@ -29,6 +29,8 @@
 // once per launch shape and kept on the context: the kernel reads its
 // arguments from a device-resident block that each call rewrites, so a later
 // call with the same launch shape replays the graph without re-capturing.
+// On the legacy or per-thread default stream, which cannot be captured, the
+// two are launched directly.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -714,8 +716,18 @@ int dt_hooi_batched(dt_ctx *ctx, int count, const int64_t *shapes, const int64_t
         // captured once, replayed by every later call.
         const std::pair<int, unsigned> gkey(nt, grid);
         int reused = 1;
-        auto itg = st.graphs.find(gkey);
-        if (itg == st.graphs.end()) {
+        // Streams that cannot be captured (the legacy and per-thread default
+        // streams) run the launch directly.
+        const bool capturable = ctx->stream != nullptr && ctx->stream != cudaStreamLegacy &&
+                                ctx->stream != cudaStreamPerThread;
+        if (!capturable) {
+            DT_CUDA(cudaEventRecord(ctx->ev_start, ctx->stream));
+            enqueue_kernel(ctx, nt, grid, st.args.as<BatchArgs>(), st.queue.as<int>());
+            DT_CUDA(cudaEventRecord(ctx->ev_stop, ctx->stream));
+            reused = 0;
+        }
+        auto itg = capturable ? st.graphs.find(gkey) : st.graphs.end();
+        if (capturable && itg == st.graphs.end()) {
             reused = 0;
             cudaGraph_t graph;
             cudaGraphExec_t exec;
@@ -734,10 +746,12 @@ int dt_hooi_batched(dt_ctx *ctx, int count, const int64_t *shapes, const int64_t
             DT_CUDA(ie);
             itg = st.graphs.emplace(gkey, exec).first;
         }
-        DT_CUDA(cudaEventRecord(ctx->ev_start, ctx->stream));
-        DT_CUDA(cudaGraphLaunch(itg->second, ctx->stream));
-        ctx->launches++;
-        DT_CUDA(cudaEventRecord(ctx->ev_stop, ctx->stream));
+        if (capturable) {
+            DT_CUDA(cudaEventRecord(ctx->ev_start, ctx->stream));
+            DT_CUDA(cudaGraphLaunch(itg->second, ctx->stream));
+            ctx->launches++;
+            DT_CUDA(cudaEventRecord(ctx->ev_stop, ctx->stream));
+        }
         DT_CUDA(cudaStreamSynchronize(ctx->stream));
         float ms = 0.f;
         DT_CUDA(cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop));

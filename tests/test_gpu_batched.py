@@ -122,3 +122,23 @@ def test_batched_4096_configured_batch_vs_reference(ctx, oracle_ref):
                 worst_ang = max(worst_ang, dense.principal_angle_max(U[t][n], Ur[n]))
     assert worst_res <= 1e-10, worst_res
     assert worst_ang <= 1e-8, worst_ang
+
+
+def test_batched_on_the_legacy_default_stream(ctx):
+    """torch CUDA buffers on torch's default (legacy) stream: the launch cannot
+    be captured there and runs directly, with the same results."""
+    import torch
+    items, U0 = _batch(24, 7)
+    tensors = [X for X, _ in items]
+    ranks = [r for _, r in items]
+    U1, G1, e1, _ = ctx.hooi_batched(tensors, ranks, U0, sweeps=4, block_threads=256)
+    pk = ctx.pack_batched(tensors, ranks, U0)
+    with torch.cuda.stream(torch.cuda.default_stream()):
+        Xd = torch.from_numpy(pk["X"]).cuda()
+        Ud = torch.from_numpy(pk["U"]).cuda()
+        Gd = torch.zeros(pk["g_size"], dtype=torch.float64, device="cuda")
+        Ed = torch.zeros(pk["count"], dtype=torch.float64, device="cuda")
+        rep = ctx.hooi_batched_packed(pk, Ud, Gd, Ed, X=Xd, sweeps=4, block_threads=256)
+        torch.cuda.synchronize()
+    assert rep["graph_reused"] == 0
+    np.testing.assert_array_equal(Ed.cpu().numpy(), e1)
