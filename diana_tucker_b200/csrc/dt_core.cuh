@@ -29,6 +29,11 @@ struct dt_ctx {
     int num_sms = 0;
     int64_t launches = 0;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    // Chunked host-to-device staging: a copy stream whose chunks the context
+    // stream waits for one by one (created on first use).
+    static constexpr int kCopyChunks = 16;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t copy_ev[kCopyChunks + 1] = {};
     // The dense HOOI drivers' last plans (device buffers plus a captured graph
     // of one sweep), reused by the next call with the same shapes, ranks and
     // options; released before the stream at dt_ctx_destroy.

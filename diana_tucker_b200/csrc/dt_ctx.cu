@@ -219,6 +219,12 @@ int dt_ctx_destroy(dt_ctx *ctx) {
         if (ctx->stream) cudaStreamSynchronize(ctx->stream);
         if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
         if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
+        if (ctx->copy_stream) {
+            cudaStreamSynchronize(ctx->copy_stream);
+            for (cudaEvent_t e : ctx->copy_ev)
+                if (e) cudaEventDestroy(e);
+            cudaStreamDestroy(ctx->copy_stream);
+        }
         if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
         delete ctx;
     });

@@ -427,7 +427,12 @@ int dt_hooi_dense(dt_ctx *ctx, const void *X, int dtype, int ndim, const int64_t
         DT_CUDA(cudaSetDevice(ctx->device));
         if (report) std::memset(report, 0, sizeof(*report));
         const size_t esz = dtype == DT_F64 ? 8 : 4;
-        DevView x(ctx, X, prod(shape, ndim) * esz, true, false);
+        // A host FP32 X of the tensor-core path is copied in chunks by that
+        // path (the copy overlaps its rounding to BF16); any other host X is
+        // staged here.
+        const bool x_host = o.precision != DT_PREC_FP64 && dtype == DT_F32 && !is_device_ptr(X) &&
+                            hooi_lowprec_tc_ok(ndim, shape, ranks);
+        DevView x(ctx, x_host ? nullptr : X, x_host ? 0 : prod(shape, ndim) * esz, true, false);
         SummaryScope sc(ctx, "Algorithm::Tucker::HOOI_ALS()");
         if (o.precision == DT_PREC_FP64) {
             // A staged host X lives only for this call: its plan is not kept
@@ -442,7 +447,8 @@ int dt_hooi_dense(dt_ctx *ctx, const void *X, int dtype, int ndim, const int64_t
             plan->h.setup(ctx, x.ptr(), dtype, ndim, shape, ranks, o);
             plan->h.run(G, U, report, keep ? &plan->graph : nullptr);
         } else {
-            hooi_dense_lowprec(ctx, x.ptr(), dtype, ndim, shape, ranks, o, G, U, report);
+            hooi_dense_lowprec(ctx, x_host ? X : x.ptr(), dtype, ndim, shape, ranks, o, G, U,
+                               report, x_host);
         }
     });
 }

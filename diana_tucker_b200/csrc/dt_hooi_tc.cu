@@ -237,7 +237,7 @@ struct MixedHooi {
     }
 
     void run(const void *X, int dtype, double *G_user, double *const *U_user,
-             dt_hooi_report *rep) {
+             dt_hooi_report *rep, bool x_host) {
         const int64_t launches0 = ctx->launches;
         LaunchTimer timer(ctx, opts.profile != 0);
         xtimer = &timer;
@@ -248,7 +248,10 @@ struct MixedHooi {
                                 (opts.precision == DT_PREC_BF16 && opts.refine_sweeps > 0);
         xsplit = want_split;
         DT_CUDA(cudaEventRecord(ctx->ev_start, ctx->stream));
-        if (dtype == DT_F32) {
+        if (x_host) {
+            X32own.alloc(ctx, xsize * sizeof(float));
+            X32 = X32own.as<float>();
+        } else if (dtype == DT_F32) {
             X32 = static_cast<const float *>(X);
         } else {
             X32own.alloc(ctx, xsize * sizeof(float));
@@ -263,9 +266,14 @@ struct MixedHooi {
         if (dtype == DT_F64)
             sumsq(ctx, X, DT_F64, xsize, scal.as<double>());
         DevMem x2f(ctx, sizeof(double));
-        split_f32(ctx, X32, xsize, Xh.as<__nv_bfloat16>(),
-                  want_split ? Xl.as<__nv_bfloat16>() : nullptr,
-                  dtype == DT_F32 ? scal.as<double>() : x2f.as<double>());
+        if (x_host)
+            split_f32_from_host(ctx, static_cast<const float *>(X), xsize, X32own.as<float>(),
+                                Xh.as<__nv_bfloat16>(),
+                                want_split ? Xl.as<__nv_bfloat16>() : nullptr, scal.as<double>());
+        else
+            split_f32(ctx, X32, xsize, Xh.as<__nv_bfloat16>(),
+                      want_split ? Xl.as<__nv_bfloat16>() : nullptr,
+                      dtype == DT_F32 ? scal.as<double>() : x2f.as<double>());
         // Initial factors: the FP64 driver's generators (libc Gaussian + QR,
         // or the caller's); HOSVD is not offered on this path.
         helper.init_factors(U_user);
@@ -402,6 +410,9 @@ struct MixedHooi {
                                 cudaMemcpyDeviceToHost, ctx->stream));
         DT_CUDA(cudaMemcpyAsync(&herr, err.get(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         DT_CUDA(cudaStreamSynchronize(ctx->stream));
+        // The FP32 copy of a host or FP64 X lives for this call only.
+        X32own.release();
+        X32 = nullptr;
         if (herr) fail(DT_ERR_CUDA, fmt("tensor-core kernel reported error %d (wait timed out)", herr));
         float ms = 0.f;
         DT_CUDA(cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop));
@@ -445,9 +456,13 @@ struct MixedPlan {
 
 }  // namespace
 
+bool hooi_lowprec_tc_ok(int ndim, const int64_t *shape, const int64_t *ranks) {
+    return MixedHooi::plan_ok_for(ndim, shape, ranks);
+}
+
 void hooi_dense_lowprec(dt_ctx *ctx, const void *X, int dtype, int ndim, const int64_t *shape,
                         const int64_t *ranks, const dt_hooi_opts &opts, double *G,
-                        double *const *U, dt_hooi_report *report) {
+                        double *const *U, dt_hooi_report *report, bool x_host) {
     DT_CHECK_ARG(opts.precision == DT_PREC_BF16 || opts.precision == DT_PREC_BF16X2 ||
                      opts.precision == DT_PREC_BF16XH,
                  "unknown precision %d", opts.precision);
@@ -500,7 +515,7 @@ void hooi_dense_lowprec(dt_ctx *ctx, const void *X, int dtype, int ndim, const i
     h.helper.setup(ctx, X, dtype, ndim, shape, ranks, opts);
     DT_CUDA(cudaMemsetAsync(h.flag.get(), 0, sizeof(int), ctx->stream));
     DT_CUDA(cudaMemsetAsync(h.err.get(), 0, sizeof(int), ctx->stream));
-    h.run(X, dtype, G, U, report);
+    h.run(X, dtype, G, U, report, x_host);
 }
 
 }  // namespace dt
