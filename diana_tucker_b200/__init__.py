@@ -122,6 +122,22 @@ class Context:
     def kernel_launches(self) -> int:
         return int(self.lib.dt_ctx_kernel_launches(self.h))
 
+    def set_mem_limit(self, nbytes: int):
+        """Caps the device memory this context's calls allocate (0: no cap);
+        a call that would cross it raises DTError(DT_ERR_NOMEM)."""
+        _lib.check(self.lib.dt_ctx_set_mem_limit(self.h, ctypes.c_uint64(int(nbytes))))
+
+    def mem_usage(self):
+        """(bytes held now, most bytes held since creation)."""
+        a, b = ctypes.c_uint64(0), ctypes.c_uint64(0)
+        _lib.check(self.lib.dt_ctx_mem_usage(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return int(a.value), int(b.value)
+
+    def selftest_wait_timeout(self, limit_cycles: int):
+        """Runs the bounded-wait self-test kernel; raises DTError(DT_ERR_TIMEOUT)
+        when its wait ran out (it always does: nothing arrives on it)."""
+        _lib.check(self.lib.dt_selftest_wait_timeout(self.h, ctypes.c_int64(int(limit_cycles))))
+
     # -- operators -----------------------------------------------------------
     def ttm(self, X, M, n: int):
         """Y = X x_n M (Function::ttm)."""

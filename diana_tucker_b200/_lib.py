@@ -18,6 +18,7 @@ DT_ERR_CUDA = 2
 DT_ERR_NOMEM = 3
 DT_ERR_NUMERIC = 4
 DT_ERR_UNSUPPORTED = 5
+DT_ERR_TIMEOUT = 6
 
 DT_F64 = 0
 DT_F32 = 1
@@ -109,6 +110,10 @@ _SIGS = [
     ("dt_ctx_synchronize", ctypes.c_int, [_vp]),
     ("dt_last_error", ctypes.c_char_p, []),
     ("dt_ctx_kernel_launches", ctypes.c_int64, [_vp]),
+    ("dt_ctx_set_mem_limit", ctypes.c_int, [_vp, ctypes.c_uint64]),
+    ("dt_ctx_mem_usage", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64),
+                                        ctypes.POINTER(ctypes.c_uint64)]),
+    ("dt_selftest_wait_timeout", ctypes.c_int, [_vp, ctypes.c_int64]),
     ("dt_ttm_f64", ctypes.c_int, [_vp, _vp, ctypes.c_int, c_i64p, ctypes.c_int, _vp,
                                   ctypes.c_int64, _vp]),
     ("dt_gram_f64", ctypes.c_int, [_vp, _vp, ctypes.c_int, c_i64p, ctypes.c_int, _vp]),

@@ -403,7 +403,9 @@ __device__ void hooi_one(const BatchArgs &a, int t, double *sm, double *T, const
         g2 = fma(acc, acc, g2);
     }
     g2 = gsum(g2, red, g);
-    if (g.lt == 0) a.relerr[t] = sqrt(fmax(0.0, 1.0 - g2 / x2));
+    // A non-finite input gives a NaN error (fmax would turn NaN into 0).
+    const double q = 1.0 - g2 / x2;
+    if (g.lt == 0) a.relerr[t] = isnan(q) ? q : sqrt(fmax(0.0, q));
     for (int e = g.lt; e < I0 * R0; e += g.gs) ug[0][e] = U0[e];
     for (int e = g.lt; e < I1 * R1; e += g.gs) ug[1][e] = U1[e];
     for (int e = g.lt; e < I2 * R2; e += g.gs) ug[2][e] = U2[e];

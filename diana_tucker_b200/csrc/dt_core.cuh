@@ -29,6 +29,9 @@ struct dt_ctx {
     int num_sms = 0;
     int64_t launches = 0;
     cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    // Device bytes held through DevMem, their maximum, and the caller's cap
+    // (0: none).
+    uint64_t mem_in_use = 0, mem_peak = 0, mem_limit = 0;
     // Chunked host-to-device staging: a copy stream whose chunks the context
     // stream waits for one by one (created on first use).
     static constexpr int kCopyChunks = 16;

@@ -1,4 +1,5 @@
 // Context lifetime, error reporting and host/device staging.
+#include <algorithm>
 #include <cstdlib>
 #include <map>
 #include <mutex>
@@ -94,6 +95,19 @@ void SweepGraph::run(dt_ctx *ctx, const std::function<void()> &fn) {
         cudaGraph_t g = nullptr;
         try {
             fn();
+        } catch (const Error &e) {
+            cudaStreamEndCapture(ctx->stream, &g);
+            if (e.code == DT_ERR_NOMEM) {
+                // Out of memory (or over the context's cap): the call fails and
+                // the next one captures again.
+                if (g) cudaGraphDestroy(g);
+                cudaGetLastError();
+                ctx->launches = l0;
+                throw;
+            }
+            give_up(g);
+            fn();
+            return;
         } catch (...) {
             cudaStreamEndCapture(ctx->stream, &g);
             give_up(g);
@@ -131,14 +145,32 @@ void raise_smem_limit(dt_ctx *ctx, const void *kernel, size_t bytes) {
 
 void DevMem::alloc(dt_ctx *ctx, size_t bytes) {
     release();
+    if (bytes == 0) return;
+    if (ctx->mem_limit && ctx->mem_in_use + bytes > ctx->mem_limit)
+        fail(DT_ERR_NOMEM, fmt("device allocation of %zu bytes would exceed the context's "
+                               "limit (%llu of %llu bytes in use)",
+                               bytes, (unsigned long long)ctx->mem_in_use,
+                               (unsigned long long)ctx->mem_limit));
+    const cudaError_t e = cudaMallocAsync(&p_, bytes, ctx->stream);
+    if (e != cudaSuccess) {
+        p_ = nullptr;
+        if (e == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            fail(DT_ERR_NOMEM, fmt("device allocation of %zu bytes failed", bytes));
+        }
+        DT_CUDA(e);
+    }
     ctx_ = ctx;
     bytes_ = bytes;
-    if (bytes == 0) return;
-    DT_CUDA(cudaMallocAsync(&p_, bytes, ctx->stream));
+    ctx->mem_in_use += bytes;
+    ctx->mem_peak = std::max(ctx->mem_peak, ctx->mem_in_use);
 }
 
 void DevMem::release() {
-    if (p_ && ctx_) cudaFreeAsync(p_, ctx_->stream);
+    if (p_ && ctx_) {
+        cudaFreeAsync(p_, ctx_->stream);
+        ctx_->mem_in_use -= bytes_;
+    }
     p_ = nullptr;
     bytes_ = 0;
 }
@@ -234,6 +266,21 @@ int dt_ctx_set_stream(dt_ctx *ctx, void *stream) {
     return guard([&] {
         check_ctx(ctx);
         ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+    });
+}
+
+int dt_ctx_set_mem_limit(dt_ctx *ctx, uint64_t bytes) {
+    return guard([&] {
+        check_ctx(ctx);
+        ctx->mem_limit = bytes;
+    });
+}
+
+int dt_ctx_mem_usage(dt_ctx *ctx, uint64_t *in_use, uint64_t *peak) {
+    return guard([&] {
+        check_ctx(ctx);
+        if (in_use) *in_use = ctx->mem_in_use;
+        if (peak) *peak = ctx->mem_peak;
     });
 }
 

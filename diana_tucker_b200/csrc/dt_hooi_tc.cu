@@ -413,7 +413,7 @@ struct MixedHooi {
         // The FP32 copy of a host or FP64 X lives for this call only.
         X32own.release();
         X32 = nullptr;
-        if (herr) fail(DT_ERR_CUDA, fmt("tensor-core kernel reported error %d (wait timed out)", herr));
+        if (herr) fail(DT_ERR_TIMEOUT, fmt("tensor-core kernel reported error %d (wait timed out)", herr));
         float ms = 0.f;
         DT_CUDA(cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop));
         if (!std::isfinite(g2)) fail(DT_ERR_NUMERIC, "HOOI produced a non-finite core");

@@ -1,11 +1,47 @@
 // extern "C" entry points for the tensor-core operators on their own
 // (mixed-precision TTM and Gram), used by the HOOI driver internally.
 #include "dt_kernels.cuh"
+#include "dt_tc.cuh"
 #include "dt_tc_host.cuh"
 
 using namespace dt;
 
+namespace {
+
+// One mbarrier that nothing arrives on: every thread's bounded wait runs out,
+// records the timeout in the error word, and the kernel returns.  No copy or
+// MMA is issued, so nothing is in flight when it exits.
+__global__ void wait_selftest_kernel(int *err, long long limit) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        tc::mbar_init(&bar, 1);
+        tc::fence_mbar_init();
+    }
+    __syncthreads();
+    tc::mbar_wait(&bar, 0, err, limit);
+}
+
+}  // namespace
+
 extern "C" {
+
+int dt_selftest_wait_timeout(dt_ctx *ctx, int64_t limit_cycles) {
+    return guard([&] {
+        check_ctx(ctx);
+        DT_CHECK_ARG(limit_cycles >= 0 && limit_cycles <= tc::kWaitCycles,
+                     "dt_selftest_wait_timeout: limit %lld outside [0, %lld]",
+                     (long long)limit_cycles, (long long)tc::kWaitCycles);
+        DT_CUDA(cudaSetDevice(ctx->device));
+        DevMem err(ctx, sizeof(int));
+        DT_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(int), ctx->stream));
+        DT_LAUNCH(ctx, wait_selftest_kernel, 1, 32, 0, err.as<int>(), (long long)limit_cycles);
+        int h = 0;
+        DT_CUDA(cudaMemcpyAsync(&h, err.get(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        DT_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (h) fail(DT_ERR_TIMEOUT, fmt("self-test: the bounded wait ran out after %lld cycles "
+                                        "(error word %d)", (long long)limit_cycles, h));
+    });
+}
 
 int dt_ttm_tc(dt_ctx *ctx, const float *X, int ndim, const int64_t *shape, int mode,
               const double *U, int64_t J, int split, float *Y) {
@@ -44,7 +80,7 @@ int dt_ttm_tc(dt_ctx *ctx, const float *X, int ndim, const int64_t *shape, int m
         int h = 0;
         DT_CUDA(cudaMemcpyAsync(&h, err.get(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         DT_CUDA(cudaStreamSynchronize(ctx->stream));
-        if (h) fail(DT_ERR_CUDA, "dt_ttm_tc: a tensor-core wait timed out");
+        if (h) fail(DT_ERR_TIMEOUT, "dt_ttm_tc: a tensor-core wait timed out");
         y.finish();
     });
 }
@@ -69,7 +105,7 @@ int dt_gram_tc(dt_ctx *ctx, const float *Y, int64_t I, int64_t K, int split, dou
         int h = 0;
         DT_CUDA(cudaMemcpyAsync(&h, err.get(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         DT_CUDA(cudaStreamSynchronize(ctx->stream));
-        if (h) fail(DT_ERR_CUDA, "dt_gram_tc: a tensor-core wait timed out");
+        if (h) fail(DT_ERR_TIMEOUT, "dt_gram_tc: a tensor-core wait timed out");
         s.finish();
     });
 }

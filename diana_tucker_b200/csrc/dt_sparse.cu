@@ -1546,6 +1546,7 @@ int dt_sp_hooi(dt_ctx *ctx, const dt_sptensor *sp, const int64_t *R, int max_swe
         }
         for (auto &v : views) v.finish();
         DT_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (!std::isfinite(hg2)) fail(DT_ERR_NUMERIC, "sparse HOOI produced a non-finite core");
         float ms = 0.f;
         DT_CUDA(cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop));
         if (report) {

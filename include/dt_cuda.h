@@ -40,6 +40,8 @@ extern "C" {
 #define DT_ERR_NOMEM 3     /* device allocation failed */
 #define DT_ERR_NUMERIC 4   /* breakdown (singular matrix, non-SPD Gram, NaN) */
 #define DT_ERR_UNSUPPORTED 5
+#define DT_ERR_TIMEOUT 6   /* a bounded device wait ran out: the kernel recorded it
+                              and returned, and the context stays usable */
 
 /* ---- element types and options --------------------------------------- */
 #define DT_F64 0
@@ -110,6 +112,19 @@ DT_API int dt_ctx_synchronize(dt_ctx *ctx);
 DT_API const char *dt_last_error(void);
 /* Number of this library's kernels launched by ctx since creation. */
 DT_API int64_t dt_ctx_kernel_launches(dt_ctx *ctx);
+/* A cap on the device memory this context's calls allocate (bytes; 0 = no
+ * cap).  A call whose allocation would cross it fails with DT_ERR_NOMEM before
+ * allocating, frees what it holds and leaves the context usable (the
+ * reference's Operator::alloc ends the process instead, operator_cpu.tpp:6-12). */
+DT_API int dt_ctx_set_mem_limit(dt_ctx *ctx, uint64_t bytes);
+/* Device bytes the context holds now (cached plans included) and at most
+ * since creation. */
+DT_API int dt_ctx_mem_usage(dt_ctx *ctx, uint64_t *in_use, uint64_t *peak);
+/* Self-test of the bounded device waits: one kernel waits on an mbarrier that
+ * nothing arrives on, for limit_cycles SM clock cycles (<= the 2e9 budget of
+ * every wait in the library), records the timeout and returns.  Returns
+ * DT_ERR_TIMEOUT, as a real wait that ran out does; the context stays usable. */
+DT_API int dt_selftest_wait_timeout(dt_ctx *ctx, int64_t limit_cycles);
 
 /* ---- operator-level entry points -------------------------------------- */
 /* Y = X x_mode M, M is J x I_mode col-major, Y has shape[mode] replaced by J.
