@@ -449,7 +449,7 @@ def run_ours(args):
                 "d2h_bytes_per_step": int(d2h), "h2d_bare_ms": round(h2d_ms, 4),
                 "h2d_bare_gbs": round(h2d / h2d_ms / 1e6, 1) if h2d_ms > 0 else None,
                 "above_bare_h2d_ms": round(e2e_ms - h2d_ms, 4),
-                "overlap": "X copied in 16 chunks on a copy stream; each chunk rounded to "
+                "overlap": "X copied in 4 chunks on a copy stream, issued first; each chunk rounded to "
                            "BF16 (and summed into ||X||^2) as it lands; the sweeps need "
                            "all of X"},
         "gpu_launches": int(launches // max(1, args.steps)),

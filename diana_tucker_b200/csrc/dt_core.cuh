@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
@@ -34,7 +35,7 @@ struct dt_ctx {
     uint64_t mem_in_use = 0, mem_peak = 0, mem_limit = 0;
     // Chunked host-to-device staging: a copy stream whose chunks the context
     // stream waits for one by one (created on first use).
-    static constexpr int kCopyChunks = 16;
+    static constexpr int kCopyChunks = 4;
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t copy_ev[kCopyChunks + 1] = {};
     // The dense HOOI drivers' last plans (device buffers plus a captured graph
@@ -237,6 +238,20 @@ class DevMem {
     void *p_ = nullptr;
     size_t bytes_ = 0;
     dt_ctx *ctx_ = nullptr;
+};
+
+// A host buffer copied to a new device buffer in ctx->kCopyChunks chunks on
+// the context's copy stream (created on first use), all issued by start();
+// wait(c) makes the context stream wait for chunk c.  Chunks are multiples of
+// 1024 elements of `esz` bytes.
+struct ChunkedUpload {
+    DevMem dst;
+    int64_t n = 0, step = 0;
+    int chunks = 0;
+    void start(dt_ctx *ctx, const void *host, int64_t n, size_t esz);
+    void wait(dt_ctx *ctx, int c) const;
+    int64_t offset(int c) const { return (int64_t)c * step; }
+    int64_t length(int c) const { return std::min(step, n - offset(c)); }
 };
 
 // A caller buffer seen from the device: device pointers pass through, host

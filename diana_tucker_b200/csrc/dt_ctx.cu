@@ -175,6 +175,32 @@ void DevMem::release() {
     bytes_ = 0;
 }
 
+void ChunkedUpload::start(dt_ctx *c, const void *host, int64_t count, size_t esz) {
+    constexpr int kc = dt_ctx::kCopyChunks;
+    if (!c->copy_stream) {
+        DT_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        for (cudaEvent_t &e : c->copy_ev)
+            DT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    n = count;
+    step = std::max<int64_t>(1024, ((n + kc - 1) / kc + 1023) / 1024 * 1024);
+    chunks = (int)((n + step - 1) / step);
+    dst.alloc(c, (size_t)n * esz);
+    // The copies follow the context stream's earlier work (dst's allocation).
+    DT_CUDA(cudaEventRecord(c->copy_ev[kc], c->stream));
+    DT_CUDA(cudaStreamWaitEvent(c->copy_stream, c->copy_ev[kc], 0));
+    for (int q = 0; q < chunks; q++) {
+        DT_CUDA(cudaMemcpyAsync(static_cast<char *>(dst.get()) + offset(q) * esz,
+                                static_cast<const char *>(host) + offset(q) * esz,
+                                (size_t)length(q) * esz, cudaMemcpyHostToDevice, c->copy_stream));
+        DT_CUDA(cudaEventRecord(c->copy_ev[q], c->copy_stream));
+    }
+}
+
+void ChunkedUpload::wait(dt_ctx *c, int q) const {
+    DT_CUDA(cudaStreamWaitEvent(c->stream, c->copy_ev[q], 0));
+}
+
 DevView::DevView(dt_ctx *ctx, const void *p, size_t bytes, bool is_input, bool is_output)
     : ctx_(ctx), user_(const_cast<void *>(p)), dptr_(nullptr), bytes_(bytes),
       output_(is_output), staged_(false) {

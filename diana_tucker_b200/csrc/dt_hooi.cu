@@ -427,11 +427,13 @@ int dt_hooi_dense(dt_ctx *ctx, const void *X, int dtype, int ndim, const int64_t
         DT_CUDA(cudaSetDevice(ctx->device));
         if (report) std::memset(report, 0, sizeof(*report));
         const size_t esz = dtype == DT_F64 ? 8 : 4;
-        // A host FP32 X of the tensor-core path is copied in chunks by that
-        // path (the copy overlaps its rounding to BF16); any other host X is
-        // staged here.
+        // A host FP32 X of the tensor-core path is copied in chunks, all
+        // issued here, before any set-up; that path rounds each chunk to BF16
+        // as it lands.  Any other host X is staged in one copy.
         const bool x_host = o.precision != DT_PREC_FP64 && dtype == DT_F32 && !is_device_ptr(X) &&
                             hooi_lowprec_tc_ok(ndim, shape, ranks);
+        ChunkedUpload up;
+        if (x_host) up.start(ctx, X, prod(shape, ndim), sizeof(float));
         DevView x(ctx, x_host ? nullptr : X, x_host ? 0 : prod(shape, ndim) * esz, true, false);
         SummaryScope sc(ctx, "Algorithm::Tucker::HOOI_ALS()");
         if (o.precision == DT_PREC_FP64) {
@@ -447,8 +449,8 @@ int dt_hooi_dense(dt_ctx *ctx, const void *X, int dtype, int ndim, const int64_t
             plan->h.setup(ctx, x.ptr(), dtype, ndim, shape, ranks, o);
             plan->h.run(G, U, report, keep ? &plan->graph : nullptr);
         } else {
-            hooi_dense_lowprec(ctx, x_host ? X : x.ptr(), dtype, ndim, shape, ranks, o, G, U,
-                               report, x_host);
+            hooi_dense_lowprec(ctx, x_host ? up.dst.get() : x.ptr(), dtype, ndim, shape, ranks, o,
+                               G, U, report, x_host ? &up : nullptr);
         }
     });
 }

@@ -49,11 +49,12 @@ struct DenseHooi {
 };
 
 // BF16 / split-BF16 tensor-core HOOI (dt_hooi_tc.cu).
-// x_host: X is an FP32 host buffer, copied in chunks that overlap its
-// rounding to BF16 (only where hooi_lowprec_tc_ok holds).
+// upload: X (FP32) is still arriving from the host through it; its chunks
+// are rounded to BF16 as they land (only where hooi_lowprec_tc_ok holds).
 void hooi_dense_lowprec(dt_ctx *ctx, const void *X, int dtype, int ndim, const int64_t *shape,
                         const int64_t *ranks, const dt_hooi_opts &opts, double *G,
-                        double *const *U, dt_hooi_report *report, bool x_host = false);
+                        double *const *U, dt_hooi_report *report,
+                        ChunkedUpload *upload = nullptr);
 // Whether the tensor-core HOOI runs these shapes (otherwise it falls back to
 // the FP64 engine).
 bool hooi_lowprec_tc_ok(int ndim, const int64_t *shape, const int64_t *ranks);

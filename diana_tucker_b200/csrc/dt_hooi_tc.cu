@@ -237,7 +237,7 @@ struct MixedHooi {
     }
 
     void run(const void *X, int dtype, double *G_user, double *const *U_user,
-             dt_hooi_report *rep, bool x_host) {
+             dt_hooi_report *rep, const ChunkedUpload *upload) {
         const int64_t launches0 = ctx->launches;
         LaunchTimer timer(ctx, opts.profile != 0);
         xtimer = &timer;
@@ -248,10 +248,7 @@ struct MixedHooi {
                                 (opts.precision == DT_PREC_BF16 && opts.refine_sweeps > 0);
         xsplit = want_split;
         DT_CUDA(cudaEventRecord(ctx->ev_start, ctx->stream));
-        if (x_host) {
-            X32own.alloc(ctx, xsize * sizeof(float));
-            X32 = X32own.as<float>();
-        } else if (dtype == DT_F32) {
+        if (dtype == DT_F32) {
             X32 = static_cast<const float *>(X);
         } else {
             X32own.alloc(ctx, xsize * sizeof(float));
@@ -266,10 +263,9 @@ struct MixedHooi {
         if (dtype == DT_F64)
             sumsq(ctx, X, DT_F64, xsize, scal.as<double>());
         DevMem x2f(ctx, sizeof(double));
-        if (x_host)
-            split_f32_from_host(ctx, static_cast<const float *>(X), xsize, X32own.as<float>(),
-                                Xh.as<__nv_bfloat16>(),
-                                want_split ? Xl.as<__nv_bfloat16>() : nullptr, scal.as<double>());
+        if (upload)
+            split_f32_chunks(ctx, *upload, Xh.as<__nv_bfloat16>(),
+                             want_split ? Xl.as<__nv_bfloat16>() : nullptr, scal.as<double>());
         else
             split_f32(ctx, X32, xsize, Xh.as<__nv_bfloat16>(),
                       want_split ? Xl.as<__nv_bfloat16>() : nullptr,
@@ -410,7 +406,7 @@ struct MixedHooi {
                                 cudaMemcpyDeviceToHost, ctx->stream));
         DT_CUDA(cudaMemcpyAsync(&herr, err.get(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         DT_CUDA(cudaStreamSynchronize(ctx->stream));
-        // The FP32 copy of a host or FP64 X lives for this call only.
+        // The FP32 copy of an FP64 X lives for this call only.
         X32own.release();
         X32 = nullptr;
         if (herr) fail(DT_ERR_TIMEOUT, fmt("tensor-core kernel reported error %d (wait timed out)", herr));
@@ -462,7 +458,7 @@ bool hooi_lowprec_tc_ok(int ndim, const int64_t *shape, const int64_t *ranks) {
 
 void hooi_dense_lowprec(dt_ctx *ctx, const void *X, int dtype, int ndim, const int64_t *shape,
                         const int64_t *ranks, const dt_hooi_opts &opts, double *G,
-                        double *const *U, dt_hooi_report *report, bool x_host) {
+                        double *const *U, dt_hooi_report *report, ChunkedUpload *upload) {
     DT_CHECK_ARG(opts.precision == DT_PREC_BF16 || opts.precision == DT_PREC_BF16X2 ||
                      opts.precision == DT_PREC_BF16XH,
                  "unknown precision %d", opts.precision);
@@ -515,7 +511,7 @@ void hooi_dense_lowprec(dt_ctx *ctx, const void *X, int dtype, int ndim, const i
     h.helper.setup(ctx, X, dtype, ndim, shape, ranks, opts);
     DT_CUDA(cudaMemsetAsync(h.flag.get(), 0, sizeof(int), ctx->stream));
     DT_CUDA(cudaMemsetAsync(h.err.get(), 0, sizeof(int), ctx->stream));
-    h.run(X, dtype, G, U, report, x_host);
+    h.run(X, dtype, G, U, report, upload);
 }
 
 }  // namespace dt

@@ -723,33 +723,20 @@ void split_f32(dt_ctx *ctx, const float *x, int64_t n, __nv_bfloat16 *hi, __nv_b
     DT_LAUNCH(ctx, sum_double_kernel, 1, 1024, 0, part.as<double>(), blocks, sumsq_out);
 }
 
-void split_f32_from_host(dt_ctx *ctx, const float *hx, int64_t n, float *dx, __nv_bfloat16 *hi,
-                         __nv_bfloat16 *lo, double *sumsq_out) {
-    constexpr int kc = dt_ctx::kCopyChunks;
-    if (!ctx->copy_stream) {
-        DT_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
-        for (cudaEvent_t &e : ctx->copy_ev)
-            DT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    }
-    // Chunks of a multiple of 1024 elements (16-byte aligned device offsets).
-    const int64_t step = std::max<int64_t>(1024, (ceil_div(n, kc) + 1023) / 1024 * 1024);
-    const int nch = (int)ceil_div(n, step);
-    const int bpc = std::max(1, std::min<int>(ctx->num_sms, (int)ceil_div(step / 4 + 1, 256)));
-    DevMem part(ctx, (size_t)nch * bpc * sizeof(double));
-    // The copies follow the context stream's earlier work (dx's allocation).
-    DT_CUDA(cudaEventRecord(ctx->copy_ev[kc], ctx->stream));
-    DT_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->copy_ev[kc], 0));
-    for (int c = 0; c < nch; c++) {
-        const int64_t off = (int64_t)c * step, len = std::min(step, n - off);
-        DT_CUDA(cudaMemcpyAsync(dx + off, hx + off, (size_t)len * sizeof(float),
-                                cudaMemcpyHostToDevice, ctx->copy_stream));
-        DT_CUDA(cudaEventRecord(ctx->copy_ev[c], ctx->copy_stream));
-        DT_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->copy_ev[c], 0));
-        DT_LAUNCH(ctx, split_f32_kernel, bpc, 256, 0, dx + off, len, hi + off,
+void split_f32_chunks(dt_ctx *ctx, const ChunkedUpload &up, __nv_bfloat16 *hi,
+                      __nv_bfloat16 *lo, double *sumsq_out) {
+    const float *dx = up.dst.as<float>();
+    const int bpc =
+        std::max(1, std::min<int>(2 * ctx->num_sms, (int)ceil_div(up.step / 4 + 1, 256)));
+    DevMem part(ctx, (size_t)up.chunks * bpc * sizeof(double));
+    for (int c = 0; c < up.chunks; c++) {
+        up.wait(ctx, c);
+        const int64_t off = up.offset(c);
+        DT_LAUNCH(ctx, split_f32_kernel, bpc, 256, 0, dx + off, up.length(c), hi + off,
                   lo ? lo + off : nullptr, part.as<double>() + (size_t)c * bpc);
     }
     // Partials in chunk order: the same sum on every call.
-    DT_LAUNCH(ctx, sum_double_kernel, 1, 1024, 0, part.as<double>(), nch * bpc, sumsq_out);
+    DT_LAUNCH(ctx, sum_double_kernel, 1, 1024, 0, part.as<double>(), up.chunks * bpc, sumsq_out);
 }
 
 void core_rows(dt_ctx *ctx, const __nv_bfloat16 *Yh, const __nv_bfloat16 *Yl, int64_t I, int64_t K,

@@ -63,10 +63,10 @@ bool tc_gram_supported(int64_t I, int64_t K);
 void tc_gram(dt_ctx *ctx, const __nv_bfloat16 *Yh, const __nv_bfloat16 *Yl, int64_t I, int64_t K,
              double *S, int *err);
 
-// The same from a host x: x is copied to dx in chunks on the context's copy
-// stream, and each chunk is rounded as soon as it has landed.
-void split_f32_from_host(dt_ctx *ctx, const float *hx, int64_t n, float *dx, __nv_bfloat16 *hi,
-                         __nv_bfloat16 *lo, double *sumsq_out);
+// The same over an FP32 upload in flight: each chunk is rounded as soon as it
+// has landed.
+void split_f32_chunks(dt_ctx *ctx, const ChunkedUpload &up, __nv_bfloat16 *hi,
+                      __nv_bfloat16 *lo, double *sumsq_out);
 void split_f32(dt_ctx *ctx, const float *x, int64_t n, __nv_bfloat16 *hi, __nv_bfloat16 *lo,
                double *sumsq_out);
 
