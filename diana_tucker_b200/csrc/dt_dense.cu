@@ -483,8 +483,8 @@ template void ttm_f64<float>(dt_ctx *, const float *, int64_t, int64_t, int64_t,
 //                                   koff(q) = (q % L) + LI*(q / L)  (unfolding)
 // This covers Function::gram / ttt_except (both operands are mode-n
 // unfoldings X_(n), q running over the other modes) and matmulNN/NT/TN.
-// 64 x 64 output tiles, 4 x 4 per thread, split-K over gridDim.z with a
-// deterministic reduction of the partial tiles.
+// 64 x 64 output tiles on the FP64 tensor cores, split-K over gridDim.z with
+// a deterministic reduction of the partial tiles.
 // ---------------------------------------------------------------------------
 namespace {
 
@@ -509,9 +509,19 @@ __device__ __forceinline__ int64_t koff(const Operand &o, int64_t q) {
 constexpr int GM_B = 64;
 constexpr int GM_BK = 16;
 constexpr int GM_NT = 256;
+// Staged rows are 68 doubles apart: the four k-rows of an mma.sync fragment
+// load (lanes g + 8 t, 64-bit loads served per half-warp) fall in different
+// banks.
+constexpr int GM_P = GM_B + 4;
 
-__device__ __forceinline__ void load_tile(double (*dst)[GM_B], const Operand &o, int64_t i0,
-                                          int64_t nI, int64_t q0, int64_t qend, int t) {
+// One thread's four elements of a 16 x 64 operand tile: fetched into
+// registers (fetch) while the previous tile is consumed, then stored (store).
+struct TileRegs {
+    double v[4];
+};
+
+__device__ __forceinline__ void fetch_tile(TileRegs &r, const Operand &o, int64_t i0, int64_t nI,
+                                           int64_t q0, int64_t qend, int t) {
     if (o.kfast) {
         // 16 consecutive q per row, 16 rows per pass.
         const int k = t & 15;
@@ -519,69 +529,101 @@ __device__ __forceinline__ void load_tile(double (*dst)[GM_B], const Operand &o,
         const bool qok = q < qend;
         const int64_t off = qok ? koff(o, q) : 0;
 #pragma unroll
-        for (int s = 0; s < GM_B / 16; s++) {
-            const int m = (t >> 4) + 16 * s;
-            const int64_t i = i0 + m;
-            dst[k][m] = (qok && i < nI) ? o.p[off + i * o.si] : 0.0;
+        for (int s = 0; s < 4; s++) {
+            const int64_t i = i0 + (t >> 4) + 16 * s;
+            r.v[s] = (qok && i < nI) ? o.p[off + i * o.si] : 0.0;
         }
     } else {
         // 64 consecutive output indices per q, 4 q per pass.
-        const int m = t & 63;
-        const int64_t i = i0 + m;
+        const int64_t i = i0 + (t & 63);
 #pragma unroll
-        for (int s = 0; s < GM_BK / 4; s++) {
-            const int k = (t >> 6) + 4 * s;
-            const int64_t q = q0 + k;
-            dst[k][m] = (q < qend && i < nI) ? o.p[koff(o, q) + i * o.si] : 0.0;
+        for (int s = 0; s < 4; s++) {
+            const int64_t q = q0 + (t >> 6) + 4 * s;
+            r.v[s] = (q < qend && i < nI) ? o.p[koff(o, q) + i * o.si] : 0.0;
         }
     }
 }
 
+__device__ __forceinline__ void store_tile(double (*dst)[GM_P], const TileRegs &r,
+                                           const Operand &o, int t) {
+    if (o.kfast) {
+#pragma unroll
+        for (int s = 0; s < 4; s++) dst[t & 15][(t >> 4) + 16 * s] = r.v[s];
+    } else {
+#pragma unroll
+        for (int s = 0; s < 4; s++) dst[(t >> 6) + 4 * s][t & 63] = r.v[s];
+    }
+}
+
+__device__ __forceinline__ void gm_dmma884(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// 64 x 64 output tile per CTA on the FP64 tensor cores (mma.sync m8n8k4):
+// warp w owns rows 32 (w % 2) .. + 31 and columns 16 (w / 2) .. + 15 as 4 x 2
+// tiles of 8 x 8.  Lane (g, t) supplies a(row g, q = t) and b(col g, q = t)
+// and holds D[row g][cols 2 t, 2 t + 1].  The next 16 q of both operands are
+// fetched into registers while the current ones are multiplied.
 __global__ void __launch_bounds__(GM_NT) gemm_kernel(Operand A, Operand B, int64_t M,
                                                      int64_t N, int64_t K, int64_t kchunk,
                                                      double *__restrict__ C, int64_t ldc,
                                                      double beta, double *__restrict__ part) {
-    __shared__ __align__(16) double As[GM_BK][GM_B];
-    __shared__ __align__(16) double Bs[GM_BK][GM_B];
-    const int t = threadIdx.x;
+    __shared__ __align__(16) double As[GM_BK][GM_P];
+    __shared__ __align__(16) double Bs[GM_BK][GM_P];
+    const int t = threadIdx.x, w = t >> 5, lane = t & 31, g = lane >> 2, t4 = lane & 3;
+    const int rb = 32 * (w & 1), cb = 16 * (w >> 1);
     const int64_t i0 = (int64_t)blockIdx.x * GM_B;
     const int64_t j0 = (int64_t)blockIdx.y * GM_B;
     const int64_t qbeg = (int64_t)blockIdx.z * kchunk;
     const int64_t qend = min(K, qbeg + kchunk);
-    const int tx = t & 15, ty = t >> 4;
-    double acc[4][4] = {};
+    double acc[4][2][2];
+#pragma unroll
+    for (int m = 0; m < 4; m++)
+#pragma unroll
+        for (int n = 0; n < 2; n++) acc[m][n][0] = acc[m][n][1] = 0.0;
+    TileRegs ra, rb_;
+    if (qbeg < qend) {
+        fetch_tile(ra, A, i0, M, qbeg, qend, t);
+        fetch_tile(rb_, B, j0, N, qbeg, qend, t);
+    }
     for (int64_t q0 = qbeg; q0 < qend; q0 += GM_BK) {
-        load_tile(As, A, i0, M, q0, qend, t);
-        load_tile(Bs, B, j0, N, q0, qend, t);
+        store_tile(As, ra, A, t);
+        store_tile(Bs, rb_, B, t);
         __syncthreads();
+        if (q0 + GM_BK < qend) {
+            fetch_tile(ra, A, i0, M, q0 + GM_BK, qend, t);
+            fetch_tile(rb_, B, j0, N, q0 + GM_BK, qend, t);
+        }
 #pragma unroll
-        for (int k = 0; k < GM_BK; k++) {
-            const double2 a01 = *reinterpret_cast<const double2 *>(&As[k][4 * tx]);
-            const double2 a23 = *reinterpret_cast<const double2 *>(&As[k][4 * tx + 2]);
-            const double2 b01 = *reinterpret_cast<const double2 *>(&Bs[k][4 * ty]);
-            const double2 b23 = *reinterpret_cast<const double2 *>(&Bs[k][4 * ty + 2]);
-            const double a[4] = {a01.x, a01.y, a23.x, a23.y};
-            const double b[4] = {b01.x, b01.y, b23.x, b23.y};
+        for (int kk = 0; kk < GM_BK / 4; kk++) {
+            const int k = 4 * kk + t4;
+            const double b0 = Bs[k][cb + g], b1 = Bs[k][cb + 8 + g];
 #pragma unroll
-            for (int u = 0; u < 4; u++)
-#pragma unroll
-                for (int v = 0; v < 4; v++) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+            for (int m = 0; m < 4; m++) {
+                const double a = As[k][rb + 8 * m + g];
+                gm_dmma884(acc[m][0][0], acc[m][0][1], a, b0);
+                gm_dmma884(acc[m][1][0], acc[m][1][1], a, b1);
+            }
         }
         __syncthreads();
     }
 #pragma unroll
-    for (int u = 0; u < 4; u++) {
-        const int64_t i = i0 + 4 * tx + u;
+    for (int m = 0; m < 4; m++) {
+        const int64_t i = i0 + rb + 8 * m + g;
         if (i >= M) continue;
 #pragma unroll
-        for (int v = 0; v < 4; v++) {
-            const int64_t j = j0 + 4 * ty + v;
-            if (j >= N) continue;
-            if (part)
-                part[(int64_t)blockIdx.z * M * N + i + M * j] = acc[u][v];
-            else
-                C[i + ldc * j] = acc[u][v] + (beta != 0.0 ? beta * C[i + ldc * j] : 0.0);
-        }
+        for (int n = 0; n < 2; n++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int64_t j = j0 + cb + 8 * n + 2 * t4 + h;
+                if (j >= N) continue;
+                if (part)
+                    part[(int64_t)blockIdx.z * M * N + i + M * j] = acc[m][n][h];
+                else
+                    C[i + ldc * j] = acc[m][n][h] + (beta != 0.0 ? beta * C[i + ldc * j] : 0.0);
+            }
     }
 }
 
