@@ -44,17 +44,20 @@ __device__ __forceinline__ void bf16_split(float v, __nv_bfloat16 &hi, __nv_bflo
     lo = __float2bfloat16_rn(v - __bfloat162float(hi));
 }
 
+// lp, bp and every extent are below 2^31 (tc_ttm_supported): the digits are
+// taken with 32-bit divisions, the offset summed in 64 bits.
 __device__ __forceinline__ int64_t out_rowbase(const OutMap &om, int64_t lp, int64_t bp) {
     int64_t off = 0;
+    uint32_t l = (uint32_t)lp, b = (uint32_t)bp;
     for (int d = 0; d < om.nl; d++) {
-        const int64_t q = lp / om.dl[d];
-        off += (lp - q * om.dl[d]) * om.sl[d];
-        lp = q;
+        const uint32_t e = (uint32_t)om.dl[d], q = l / e;
+        off += (int64_t)(l - q * e) * om.sl[d];
+        l = q;
     }
     for (int d = 0; d < om.nb; d++) {
-        const int64_t q = bp / om.db[d];
-        off += (bp - q * om.db[d]) * om.sb[d];
-        bp = q;
+        const uint32_t e = (uint32_t)om.db[d], q = b / e;
+        off += (int64_t)(b - q * e) * om.sb[d];
+        b = q;
     }
     return off;
 }
@@ -174,16 +177,22 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
                                         kc * KC_ELEMS, r0);
                     }
                 } else {
+                    // Each 64-row half of the tile holds its rows for every k
+                    // contiguously ([h][k][128 B]); one box covers up to 256
+                    // k (fewer, larger boxes stream faster than one per 64 k).
                     const int64_t mb = tile % a.nmb, b = tile / a.nmb;
                     const int l0 = (int)(mb * 128);
-                    for (int kc = 0; kc < a.kchunks; kc++)
-                        for (int h = 0; h < 2; h++) {
-                            uint8_t *d = st + kc * KC_BYTES + h * (KC_BYTES / 2);
-                            tma_load_3d(d, &map_hi, &full[s], l0 + h * 64, kc * KC_ELEMS, (int)b);
+                    for (int h = 0; h < 2; h++) {
+                        uint8_t *d = st + h * (a_one / 2);
+                        for (int kb = 0; kb < a.kboxes; kb++) {
+                            const uint32_t off = (uint32_t)kb * a.kbox_rows * 128;
+                            tma_load_3d(d + off, &map_hi, &full[s], l0 + h * 64,
+                                        kb * a.kbox_rows, (int)b);
                             if (ASPLIT)
-                                tma_load_3d(d + a_one, &map_lo, &full[s], l0 + h * 64,
-                                            kc * KC_ELEMS, (int)b);
+                                tma_load_3d(d + a_one + off, &map_lo, &full[s], l0 + h * 64,
+                                            kb * a.kbox_rows, (int)b);
                         }
+                    }
                 }
             }
             // Leave no copy in flight: wait (bounded) for every stage issued.
@@ -214,8 +223,10 @@ __global__ void __launch_bounds__(TTM_THREADS, 1)
                         ad = sdesc(st + kc * KC_BYTES + sub * 32, 16, 1024, kSwizzle128B);
                         adl = sdesc(st + a_one + kc * KC_BYTES + sub * 32, 16, 1024, kSwizzle128B);
                     } else {
-                        ad = sdesc(st + kc * KC_BYTES + sub * 2048, KC_BYTES / 2, 1024, kSwizzle128B);
-                        adl = sdesc(st + a_one + kc * KC_BYTES + sub * 2048, KC_BYTES / 2, 1024,
+                        // The second 64 rows of M sit one half-stage (a_one / 2) on.
+                        ad = sdesc(st + kc * (KC_BYTES / 2) + sub * 2048, a_one / 2, 1024,
+                                   kSwizzle128B);
+                        adl = sdesc(st + a_one + kc * (KC_BYTES / 2) + sub * 2048, a_one / 2, 1024,
                                     kSwizzle128B);
                     }
                     const uint64_t bd =
@@ -642,7 +653,11 @@ void tc_ttm(dt_ctx *ctx, const __nv_bfloat16 *Xh, const __nv_bfloat16 *Xl, int64
     } else {
         const uint64_t dims[3] = {(uint64_t)L, (uint64_t)I, (uint64_t)B};
         const uint64_t str[2] = {(uint64_t)L * 2, (uint64_t)L * I * 2};
-        const uint32_t box[3] = {64, KC_ELEMS, 1};
+        // One box per half-tile over all k when the contraction is at most
+        // 256 long, else one per 64-element chunk.
+        a.kbox_rows = a.kchunks <= 4 ? a.kchunks * KC_ELEMS : KC_ELEMS;
+        a.kboxes = a.kchunks * KC_ELEMS / a.kbox_rows;
+        const uint32_t box[3] = {64, (uint32_t)a.kbox_rows, 1};
         mh = make_map(Xh, 3, dims, str, box);
         ml = Xl ? make_map(Xl, 3, dims, str, box) : mh;
     }

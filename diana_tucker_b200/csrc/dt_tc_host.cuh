@@ -25,6 +25,7 @@ struct TcTtmArgs {
     int J, Jpad, Npad;
     int split;  // A = hi + lo, B = [U_hi | U_lo]
     int kchunks, ksteps;
+    int kbox_rows, kboxes;  // MN-major: k rows per TMA box, boxes per half-tile
     int64_t nmb, ntiles;
     int stages;
     uint32_t tx_bytes;
