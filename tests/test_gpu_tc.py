@@ -100,3 +100,28 @@ def test_mixed_hooi_falls_back_to_fp64_outside_layout_rules(ctx):
     G, U, rep = ctx.hooi_dense(X, (3, 3, 3), init="randn", seed=1, max_sweeps=4,
                                precision=DT_PREC_BF16)
     assert rep["precision_used"] == DT_PREC_FP64
+
+
+@pytest.mark.parametrize("shape,ranks,prec", [
+    ((128, 96, 64), (32, 16, 8), "BF16XH"),        # rank 32: the 32-column TTM tiles
+    ((96, 80, 72), (12, 8, 4), "BF16X2"),          # ranks off the 16-column tile, X split
+    ((64, 16, 16, 16, 16), (8, 4, 4, 4, 4), "BF16XH"),  # five modes: a three-level tree
+])
+def test_mixed_hooi_shapes_vs_fp64_gpu(ctx, shape, ranks, prec):
+    """Uneven ranks, rank 32 and a 5-way tensor through the tensor-core HOOI:
+    the converged residual within 1e-6 of the FP64 path's from the same start,
+    factors within 1e-3 rad, and the core the FP64 projection of X (1e-12)."""
+    import diana_tucker_b200 as dtb
+    from diana_tucker_b200 import DT_PREC_FP64, datasets
+    X = datasets.tucker_dense(shape, ranks, noise_var=1e-6, seed=17, dtype=np.float32)
+    _, U64, r64 = ctx.hooi_dense(X, ranks, init="randn", seed=3, max_sweeps=40, tol=1e-10,
+                                 precision=DT_PREC_FP64)
+    p = getattr(dtb, "DT_PREC_" + prec)
+    G, U, rep = ctx.hooi_dense(X, ranks, init="randn", seed=3, max_sweeps=40, tol=1e-9,
+                               precision=p, inner_iters=2)
+    assert rep["precision_used"] == p
+    assert abs(rep["residual"] - r64["residual"]) < 1e-6
+    for n in range(len(shape)):
+        assert dense.principal_angle_max(U[n], U64[n]) < 1e-3, n
+        np.testing.assert_allclose(U[n].T @ U[n], np.eye(ranks[n]), atol=1e-12)
+    assert _nrel(G, dense.core(X.astype(np.float64), U)) < 1e-12
