@@ -22,8 +22,8 @@
 // Autotuning.  The block size (128, 256, 512 threads) and the packing (one
 // tensor per CTA; pairs, and quads, of the tensors small enough to share the
 // CTA's shared memory: largest mode <= 37, <= 21) are chosen by timing every
-// combination on a stratified sample of the batch; the choice is cached per
-// batch signature on the context.
+// combination on the batch (a stratified sample of 8192 tensors of larger
+// batches); the choice is cached per batch signature on the context.
 //
 // The launch (queue reset + persistent kernel) is a CUDA graph instantiated
 // once per launch shape and kept on the context: the kernel reads its
@@ -660,8 +660,11 @@ int dt_hooi_batched(dt_ctx *ctx, int count, const int64_t *shapes, const int64_t
                 pack = itc->second.second;
             } else {
                 // Autotune on a stratified sample (every k-th tensor of the
-                // cost order) with a scratch copy of U.
-                const int sample = std::min(count, 512);
+                // cost order) with a scratch copy of U.  The sample must fill
+                // the largest grid several times over, or configurations with
+                // few large CTAs win on the sample and lose on the batch: up
+                // to 8192 tensors, the whole batch is timed.
+                const int sample = std::min(count, 8192);
                 std::vector<int> sord;
                 for (int i = 0; i < sample; i++)
                     sord.push_back(order[(int64_t)i * count / sample]);

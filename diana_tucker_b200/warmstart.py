@@ -14,7 +14,7 @@ factors, template/algorithm/tucker/hooi_als.tpp:74-81):
 * screen and fall back: if the initial fit |X x_m U_m^T|^2 / |X|^2 is below
   the floor calibrated on the training tensors, HOSVD init is computed too
   and the better of the two starts is used;
-* finish: plain HOOI from the chosen start, judged by the sweeps it needs to
+* finish: plain HOOI from the chosen start, measured by the sweeps it needs to
   reach the converged FP64 relative error + 1e-6.
 
 The tensor family (256^3 FP32, seeds 1000-2999): factor columns are mixtures
