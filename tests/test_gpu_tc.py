@@ -125,3 +125,30 @@ def test_mixed_hooi_shapes_vs_fp64_gpu(ctx, shape, ranks, prec):
         assert dense.principal_angle_max(U[n], U64[n]) < 1e-3, n
         np.testing.assert_allclose(U[n].T @ U[n], np.eye(ranks[n]), atol=1e-12)
     assert _nrel(G, dense.core(X.astype(np.float64), U)) < 1e-12
+
+
+def test_mixed_hooi_host_input_matches_device_input(ctx):
+    """A host FP32 X reaches the tensor-core path in four chunk copies, each
+    rounded to BF16 as it lands; the same tensor already on the device goes
+    through one rounding pass.  Shape with a ragged last chunk (658944
+    elements, not a multiple of 4 x 1024): factors and core bit-identical,
+    residual equal to rounding (||X||^2 is summed in another order)."""
+    import torch
+    from diana_tucker_b200 import DT_PREC_BF16XH, datasets
+    shape, ranks = (104, 88, 72), (8, 8, 8)
+    X = datasets.tucker_dense(shape, ranks, noise_var=1e-4, seed=21, dtype=np.float32)
+    kw = dict(init="randn", seed=4, max_sweeps=6, tol=1e-9, precision=DT_PREC_BF16XH,
+              inner_iters=2)
+    Gh, Uh, rh = ctx.hooi_dense(X, ranks, **kw)  # pageable numpy memory
+    flat = np.ascontiguousarray(X.reshape(-1, order="F"))
+    Gp, Up, rp = ctx.hooi_dense(torch.from_numpy(flat).pin_memory(), ranks, shape=shape, **kw)
+    Gd, Ud, rd = ctx.hooi_dense(torch.from_numpy(flat).cuda(), ranks, shape=shape, **kw)
+    torch.cuda.synchronize()
+    assert rh["sweeps"] == rp["sweeps"] == rd["sweeps"]
+    for G in (Gh, Gp):
+        assert np.array_equal(np.asarray(G), np.asarray(Gd))
+    for U in (Uh, Up):
+        for a, b in zip(U, Ud):
+            assert np.array_equal(np.asarray(a), np.asarray(b))
+    assert abs(rh["residual"] - rd["residual"]) < 1e-14
+    assert abs(rp["residual"] - rd["residual"]) < 1e-14
