@@ -254,6 +254,11 @@ struct ChunkedUpload {
     int64_t length(int c) const { return std::min(step, n - offset(c)); }
 };
 
+// Queues a copy of `bytes` from device memory to a caller buffer, host or
+// device (the direction from unified addressing), on ctx->stream; the caller
+// synchronises once after its last copy.
+void copy_out(dt_ctx *ctx, void *user, const void *src, size_t bytes);
+
 // A caller buffer seen from the device: device pointers pass through, host
 // pointers are staged (copied in for inputs, copied back by finish() for
 // outputs).

@@ -217,6 +217,12 @@ DevView::DevView(dt_ctx *ctx, const void *p, size_t bytes, bool is_input, bool i
         DT_CUDA(cudaMemcpyAsync(dptr_, p, bytes, cudaMemcpyHostToDevice, ctx->stream));
 }
 
+void copy_out(dt_ctx *ctx, void *user, const void *src, size_t bytes) {
+    if (bytes == 0) return;
+    if (!user) fail(DT_ERR_ARG, "null output buffer");
+    DT_CUDA(cudaMemcpyAsync(user, src, bytes, cudaMemcpyDefault, ctx->stream));
+}
+
 void DevView::finish() {
     if (output_ && staged_ && bytes_) {
         DT_CUDA(cudaMemcpyAsync(user_, dptr_, bytes_, cudaMemcpyDeviceToHost, ctx_->stream));

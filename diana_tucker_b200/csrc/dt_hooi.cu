@@ -330,21 +330,12 @@ void DenseHooi::run(double *G_user, double *const *U_user, dt_hooi_report *rep,
     float ms = 0.f;
     DT_CUDA(cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop));
     if (!std::isfinite(g2)) fail(DT_ERR_NUMERIC, "HOOI produced a non-finite core");
-    if (G_user) {
-        DevView g(ctx, G_user, prod(R, N) * sizeof(double), false, true);
-        DT_CUDA(cudaMemcpyAsync(g.ptr(), G.get(), prod(R, N) * sizeof(double),
-                                cudaMemcpyDeviceToDevice, ctx->stream));
-        g.finish();
-    }
-    if (U_user) {
-        for (int m = 0; m < N; m++) {
-            if (!U_user[m]) continue;
-            DevView u(ctx, U_user[m], I[m] * R[m] * sizeof(double), false, true);
-            DT_CUDA(cudaMemcpyAsync(u.ptr(), U[m].get(), I[m] * R[m] * sizeof(double),
-                                    cudaMemcpyDeviceToDevice, ctx->stream));
-            u.finish();
-        }
-    }
+    // Straight from the plan's buffers into the caller's (host or device),
+    // one synchronisation for all.
+    if (G_user) copy_out(ctx, G_user, G.get(), prod(R, N) * sizeof(double));
+    if (U_user)
+        for (int m = 0; m < N; m++)
+            if (U_user[m]) copy_out(ctx, U_user[m], U[m].get(), I[m] * R[m] * sizeof(double));
     DT_CUDA(cudaStreamSynchronize(ctx->stream));
     if (rep) {
         rep->sweeps = sweeps;

@@ -379,27 +379,14 @@ struct MixedHooi {
         const double *gsrc = cur.as<double>();
         const int gslot = 2;
         DT_CUDA(cudaEventRecord(ctx->ev_stop, ctx->stream));
-        // The outputs are copied before the one synchronisation that reads
-        // ||G||^2 and the kernels' error word.
-        {
-            std::vector<DevView> outs;
-            outs.reserve(N + 1);
-            if (G_user) {
-                outs.emplace_back(ctx, G_user, prod(R, N) * sizeof(double), false, true);
-                DT_CUDA(cudaMemcpyAsync(outs.back().ptr(), gsrc, prod(R, N) * sizeof(double),
-                                        cudaMemcpyDeviceToDevice, ctx->stream));
-            }
-            if (U_user) {
-                for (int m = 0; m < N; m++) {
-                    if (!U_user[m]) continue;
-                    outs.emplace_back(ctx, U_user[m], I[m] * R[m] * sizeof(double), false, true);
-                    DT_CUDA(cudaMemcpyAsync(outs.back().ptr(), U[m].get(),
-                                            I[m] * R[m] * sizeof(double),
-                                            cudaMemcpyDeviceToDevice, ctx->stream));
-                }
-            }
-            for (auto &v : outs) v.finish();
-        }
+        // The outputs are copied (host or device, straight from the plan's
+        // buffers) before the one synchronisation that reads ||G||^2 and the
+        // kernels' error word.
+        if (G_user) copy_out(ctx, G_user, gsrc, prod(R, N) * sizeof(double));
+        if (U_user)
+            for (int m = 0; m < N; m++)
+                if (U_user[m])
+                    copy_out(ctx, U_user[m], U[m].get(), I[m] * R[m] * sizeof(double));
         double g2 = 0.0;
         int herr = 0;
         DT_CUDA(cudaMemcpyAsync(&g2, scal.as<double>() + gslot, sizeof(double),
