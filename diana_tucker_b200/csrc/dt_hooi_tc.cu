@@ -29,8 +29,10 @@ __global__ void f64_to_f32_kernel(const double *__restrict__ x, int64_t n, float
         y[e] = (float)x[e];
 }
 
+// A BF16 intermediate of the sweep (hi, and lo when split), in the plan's
+// arena.
 struct BfTensor {
-    DevMem hi, lo;
+    __nv_bfloat16 *hi = nullptr, *lo = nullptr;
     int64_t shape[16];
 };
 
@@ -49,6 +51,37 @@ struct MixedHooi {
     DenseHooi helper;  // initial factors (same generators as the FP64 driver)
     LaunchTimer *xtimer = nullptr;
     SweepGraph *g_bf16 = nullptr, *g_split = nullptr;  // captured sweeps (or null)
+    // Sweep intermediates (tensors, Gram partial tiles, core partial sums) come
+    // from one per-plan buffer used as a stack and handed out in the same order
+    // every sweep, so a captured sweep sees the same addresses and holds no
+    // allocation nodes.  A dry pass of the sweep (no launches) sizes it.
+    DevMem arena;
+    size_t arena_cap = 0, arena_off = 0, arena_need = 0;
+    bool dry = false;
+
+    void *take(size_t bytes) {
+        bytes = (bytes + 255) & ~size_t(255);
+        const size_t off = arena_off;
+        arena_off += bytes;
+        arena_need = std::max(arena_need, arena_off);
+        if (dry) return nullptr;
+        if (arena_off > arena_cap)
+            fail(DT_ERR_CUDA, fmt("internal: sweep arena of %zu bytes exceeded", arena_cap));
+        return static_cast<char *>(arena.get()) + off;
+    }
+
+    // Sizes the arena for split sweeps (the larger kind) and allocates it.
+    void size_arena() {
+        const bool s0 = split;
+        split = true;
+        dry = true;
+        arena_off = arena_need = 0;
+        sweep();
+        dry = false;
+        split = s0;
+        arena.alloc(ctx, arena_need);
+        arena_cap = arena_need;
+    }
 
     static std::vector<int> order_high_first(std::vector<int> modes) {
         std::sort(modes.begin(), modes.end(), [](int a, int b) { return a > b; });
@@ -116,8 +149,8 @@ struct MixedHooi {
             BfTensor nxt;
             std::memcpy(nxt.shape, cur.shape, N * sizeof(int64_t));
             nxt.shape[m] = R[m];
-            nxt.hi.alloc(ctx, outn * sizeof(__nv_bfloat16));
-            if (split) nxt.lo.alloc(ctx, outn * sizeof(__nv_bfloat16));
+            nxt.hi = static_cast<__nv_bfloat16 *>(take(outn * sizeof(__nv_bfloat16)));
+            if (split) nxt.lo = static_cast<__nv_bfloat16 *>(take(outn * sizeof(__nv_bfloat16)));
             OutMap om;
             const bool last_of_leaf = leaf >= 0 && q + 1 == ord.size();
             if (!last_of_leaf) {
@@ -160,21 +193,21 @@ struct MixedHooi {
                 }
             }
             const bool is_x = sh == Xh.as<__nv_bfloat16>();
-            const bool from_x = xtimer && is_x;
+            const bool from_x = xtimer && is_x && !dry;
             // X is read as hi + lo only when xsplit; every other operand, U and
             // the output follow `split`.
             const __nv_bfloat16 *a_lo = split && (!is_x || xsplit) ? sl : nullptr;
             if (from_x) xtimer->begin();
-            tc_ttm(ctx, sh, a_lo, L, cur.shape[m], B, U[m].as<double>(), R[m], om,
-                   nxt.hi.as<__nv_bfloat16>(), split ? nxt.lo.as<__nv_bfloat16>() : nullptr,
-                   nullptr, err.as<int>(), split ? 1 : 0);
+            if (!dry)
+                tc_ttm(ctx, sh, a_lo, L, cur.shape[m], B, U[m].as<double>(), R[m], om, nxt.hi,
+                       split ? nxt.lo : nullptr, nullptr, err.as<int>(), split ? 1 : 0);
             if (from_x)
                 xtimer->end((double)L * cur.shape[m] * B * 2 * (a_lo ? 2 : 1) +
                             (double)L * R[m] * B * 2 * (split ? 2 : 1) +
                             (double)cur.shape[m] * R[m] * 8);
-            cur = std::move(nxt);
-            sh = cur.hi.as<__nv_bfloat16>();
-            sl = split ? cur.lo.as<__nv_bfloat16>() : nullptr;
+            cur = nxt;
+            sh = cur.hi;
+            sl = split ? cur.lo : nullptr;
         }
         return cur;
     }
@@ -183,14 +216,17 @@ struct MixedHooi {
         int64_t K = 1;
         for (int m = 0; m < N; m++)
             if (m != n) K *= R[m];
-        const __nv_bfloat16 *yh = Y.hi.as<__nv_bfloat16>();
-        const __nv_bfloat16 *yl = split ? Y.lo.as<__nv_bfloat16>() : nullptr;
-        tc_gram(ctx, yh, yl, I[n], K, S.as<double>(), err.as<int>());
+        const __nv_bfloat16 *yh = Y.hi;
+        const __nv_bfloat16 *yl = split ? Y.lo : nullptr;
+        void *gscr = take(tc_gram_scratch_bytes(I[n], K, split));
+        void *cscr = n == N - 1 ? take(core_rows_scratch_bytes(K)) : nullptr;
+        if (dry) return;
+        tc_gram(ctx, yh, yl, I[n], K, S.as<double>(), err.as<int>(), gscr);
         subspace_iter(ctx, S.as<double>(), I[n], U[n].as<double>(), R[n], opts.inner_iters,
                       work.as<double>(), flag.as<int>());
         if (n == N - 1)
             core_rows(ctx, yh, yl, I[n], K, U[n].as<double>(), R[n], Gs.as<double>(),
-                      scal.as<double>() + 1);
+                      scal.as<double>() + 1, cscr);
     }
 
     void node(int lo, int hi, const __nv_bfloat16 *Th, const __nv_bfloat16 *Tl,
@@ -202,16 +238,20 @@ struct MixedHooi {
             for (int m = lo; m < hi; m++)
                 if (m < clo || m >= chi) modes.push_back(m);
             const bool is_leaf = chi - clo == 1;
+            // The arena is a stack: what a side allocates is released once
+            // the side is done, and the next side writes over it.
+            const size_t mark = arena_off;
             BfTensor child = contract_all(Th, Tl, shape, modes, is_leaf ? clo : -1);
             if (is_leaf)
                 leaf(clo, child);
             else
-                node(clo, chi, child.hi.as<__nv_bfloat16>(),
-                     split ? child.lo.as<__nv_bfloat16>() : nullptr, child.shape);
+                node(clo, chi, child.hi, split ? child.lo : nullptr, child.shape);
+            arena_off = mark;
         }
     }
 
     void sweep() {
+        arena_off = 0;
         node(0, N, Xh.as<__nv_bfloat16>(), split && xsplit ? Xl.as<__nv_bfloat16>() : nullptr, I);
     }
 
@@ -490,6 +530,10 @@ void hooi_dense_lowprec(dt_ctx *ctx, const void *X, int dtype, int ndim, const i
         h.Gs.alloc(ctx, prod(ranks, ndim) * sizeof(double));
         h.g_bf16 = &plan->g_bf16;
         h.g_split = &plan->g_split;
+        h.opts = opts;
+        h.xsplit = opts.precision == DT_PREC_BF16X2 ||
+                   (opts.precision == DT_PREC_BF16 && opts.refine_sweeps > 0);
+        h.size_arena();
         ctx->hooi_plan_mixed = plan;
     }
     MixedHooi &h = plan->h;

@@ -61,8 +61,11 @@ void tc_ttm(dt_ctx *ctx, const __nv_bfloat16 *Xh, const __nv_bfloat16 *Xl, int64
 bool tc_gram_supported(int64_t I, int64_t K);
 // S (I x I, FP64) = Y Y^T for the K-major BF16 Y (I rows of K); with Yl the
 // hi/lo cross terms are added.
+// `scratch` (tc_gram_scratch_bytes) holds the split-K partial tiles; NULL
+// takes a stream-ordered allocation.
 void tc_gram(dt_ctx *ctx, const __nv_bfloat16 *Yh, const __nv_bfloat16 *Yl, int64_t I, int64_t K,
-             double *S, int *err);
+             double *S, int *err, void *scratch = nullptr);
+size_t tc_gram_scratch_bytes(int64_t I, int64_t K, bool split);
 
 // The same over an FP32 upload in flight: each chunk is rounded as soon as it
 // has landed.
@@ -72,7 +75,10 @@ void split_f32(dt_ctx *ctx, const float *x, int64_t n, __nv_bfloat16 *hi, __nv_b
                double *sumsq_out);
 
 // G[k + K*r] = sum_i Y[i*K + k] U[i + I*r] (FP64 accumulate), ||G||^2 -> g2_out.
+// `scratch` (core_rows_scratch_bytes) holds the per-block partial sums; NULL
+// takes a stream-ordered allocation.
 void core_rows(dt_ctx *ctx, const __nv_bfloat16 *Yh, const __nv_bfloat16 *Yl, int64_t I, int64_t K,
-               const double *U, int64_t R, double *G, double *g2_out);
+               const double *U, int64_t R, double *G, double *g2_out, void *scratch = nullptr);
+size_t core_rows_scratch_bytes(int64_t K);
 
 }  // namespace dt
