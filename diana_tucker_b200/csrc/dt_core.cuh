@@ -103,6 +103,10 @@ __device__ __forceinline__ void pdl_trigger() {
 // DT_DISABLE_PDL=1 in the environment launches these kernels in plain
 // stream order (for diagnosis).
 bool pdl_enabled();
+// DT_DISABLE_GRAPHS=1 in the environment launches every sweep directly.
+bool graphs_enabled();
+// Whether the Summary profiler is recording on ctx.
+bool summary_active(dt_ctx *ctx);
 
 template <class... KArgs, class... Args>
 void launch_pdl(dt_ctx *ctx, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,

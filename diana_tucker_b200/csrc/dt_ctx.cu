@@ -55,6 +55,8 @@ bool pdl_enabled() {
 }
 
 namespace {
+}  // namespace
+
 bool graphs_enabled() {
     static const bool on = [] {
         const char *e = std::getenv("DT_DISABLE_GRAPHS");
@@ -62,7 +64,6 @@ bool graphs_enabled() {
     }();
     return on;
 }
-}  // namespace
 
 void release_plan(dt_ctx *ctx, std::shared_ptr<void> &plan) {
     if (!plan) return;

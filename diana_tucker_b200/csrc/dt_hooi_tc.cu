@@ -29,6 +29,42 @@ __global__ void f64_to_f32_kernel(const double *__restrict__ x, int64_t n, float
         y[e] = (float)x[e];
 }
 
+// The device-side sweep loop's state: sweeps done, the last residual, and
+// the residual of every sweep.
+struct LoopState {
+    int it, pad;
+    double prev;
+    double hist[DT_MAX_HIST];
+};
+
+// End of one sweep of the device-side loop: the sweep's residual from its
+// ||G||^2 and ||X||^2, the stop rule of the host loop (residual change below
+// `thr`, or `max_sweeps` done), and the loop's condition for the next pass.
+__global__ void sweep_check_kernel(cudaGraphConditionalHandle h, const double *scal,
+                                   LoopState *st, double thr, int max_sweeps) {
+    const double x2 = scal[0], g2 = scal[1];
+    const double res = sqrt(fmax(0.0, 1.0 - g2 / x2));
+    const int it = st->it;
+    if (it < DT_MAX_HIST) st->hist[it] = res;
+    const bool stop = it + 1 >= max_sweeps || (thr > 0.0 && it > 0 && fabs(res - st->prev) < thr);
+    st->prev = res;
+    st->it = it + 1;
+    cudaGraphSetConditional(h, stop ? 0u : 1u);
+}
+
+// The whole sweep loop as one graph: a reset of the LoopState, then a WHILE
+// node whose body is one captured sweep followed by sweep_check_kernel.
+struct LoopGraph {
+    cudaGraphExec_t exec = nullptr;
+    bool failed = false;
+    int64_t launches_per_sweep = 0;
+    double thr = -1.0;
+    int max_sweeps = -1;
+    ~LoopGraph() {
+        if (exec) cudaGraphExecDestroy(exec);
+    }
+};
+
 // A BF16 intermediate of the sweep (hi, and lo when split), in the plan's
 // arena.
 struct BfTensor {
@@ -58,6 +94,78 @@ struct MixedHooi {
     DevMem arena;
     size_t arena_cap = 0, arena_off = 0, arena_need = 0;
     bool dry = false;
+    LoopGraph *loop = nullptr;  // the device-side sweep loop (or null)
+    DevMem loopst;              // its LoopState
+
+    // Builds the device-side loop for split sweeps with stop threshold `thr`
+    // and `max_sweeps`; false (and no further attempts) when the runtime
+    // refuses any step, in which case the host drives the sweeps.
+    bool build_loop(double thr, int max_sweeps) {
+        LoopGraph &lg = *loop;
+        if (lg.exec && lg.thr == thr && lg.max_sweeps == max_sweeps) return true;
+        if (lg.failed) return false;
+        if (lg.exec) {
+            cudaGraphExecDestroy(lg.exec);
+            lg.exec = nullptr;
+        }
+        if (!loopst.get()) loopst.alloc(ctx, sizeof(LoopState));
+        cudaGraph_t g = nullptr;
+        bool ok = cudaGraphCreate(&g, 0) == cudaSuccess;
+        cudaGraphConditionalHandle h = 0;
+        ok = ok && cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) ==
+                       cudaSuccess;
+        cudaGraphNode_t reset = nullptr, cond = nullptr;
+        if (ok) {
+            cudaMemsetParams mp = {};
+            mp.dst = loopst.get();
+            mp.value = 0;
+            mp.elementSize = 4;
+            mp.width = sizeof(LoopState) / 4;
+            mp.height = 1;
+            mp.pitch = 0;
+            ok = cudaGraphAddMemsetNode(&reset, g, nullptr, 0, &mp) == cudaSuccess;
+        }
+        cudaGraphNodeParams cp = {};
+        if (ok) {
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = h;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            ok = cudaGraphAddNode(&cond, g, &reset, 1, &cp) == cudaSuccess;
+        }
+        const int64_t l0 = ctx->launches;
+        if (ok) {
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            ok = cudaStreamBeginCaptureToGraph(ctx->stream, body, nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeRelaxed) == cudaSuccess;
+            if (ok) {
+                try {
+                    sweep();
+                    DT_LAUNCH(ctx, sweep_check_kernel, 1, 1, 0, h,
+                              (const double *)scal.as<double>(), loopst.as<LoopState>(), thr,
+                              max_sweeps);
+                } catch (...) {
+                    ok = false;
+                }
+                cudaGraph_t out = nullptr;
+                ok = cudaStreamEndCapture(ctx->stream, &out) == cudaSuccess && ok;
+            }
+        }
+        lg.launches_per_sweep = ctx->launches - l0;
+        ctx->launches = l0;
+        ok = ok && cudaGraphInstantiate(&lg.exec, g, 0) == cudaSuccess;
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        if (!ok) {
+            if (lg.exec) cudaGraphExecDestroy(lg.exec);
+            lg.exec = nullptr;
+            lg.failed = true;
+            return false;
+        }
+        lg.thr = thr;
+        lg.max_sweeps = max_sweeps;
+        return true;
+    }
 
     void *take(size_t bytes) {
         bytes = (bytes + 255) & ~size_t(255);
@@ -330,7 +438,19 @@ struct MixedHooi {
         int sweeps = 0, bf16_done = 0, split_done = 0;
         const bool refine_mode = opts.precision == DT_PREC_BF16;
         split = opts.precision == DT_PREC_BF16X2 || opts.precision == DT_PREC_BF16XH;
-        for (int it = 0; it < opts.max_sweeps; it++) {
+        // Split sweeps throughout: the loop and its stop test run on the
+        // device as one graph launch (no synchronisation per sweep), unless
+        // per-sweep host work is asked for (profiling, verbose output, the
+        // Summary profiler) or the stream cannot be captured.
+        const bool plain_stream = ctx->stream != nullptr && ctx->stream != cudaStreamLegacy &&
+                                  ctx->stream != cudaStreamPerThread;
+        const bool device_loop = split && !refine_mode && loop && plain_stream &&
+                                 graphs_enabled() && !opts.profile && !opts.verbose &&
+                                 !summary_active(ctx) && opts.max_sweeps >= 1 &&
+                                 build_loop(opts.tol > 0 ? std::max(opts.tol, kSplitFloor) : 0.0,
+                                            opts.max_sweeps);
+        if (device_loop) DT_CUDA(cudaGraphLaunch(loop->exec, ctx->stream));
+        for (int it = 0; it < (device_loop ? 0 : opts.max_sweeps); it++) {
             if (!split && refine_mode && opts.refine_sweeps > 0 &&
                 it >= opts.max_sweeps - opts.refine_sweeps) {
                 split = true;
@@ -384,7 +504,7 @@ struct MixedHooi {
                 }
             }
         }
-        if (x2 < 0.0) x2 = read_scalar(0);
+        if (x2 < 0.0 && !device_loop) x2 = read_scalar(0);
         // Final core, FP64 projection from the original X (the returned G is
         // X x_1 U_1^T ... x_N U_N^T to FP64 rounding).
         DevMem cur;
@@ -432,7 +552,22 @@ struct MixedHooi {
         DT_CUDA(cudaMemcpyAsync(&g2, scal.as<double>() + gslot, sizeof(double),
                                 cudaMemcpyDeviceToHost, ctx->stream));
         DT_CUDA(cudaMemcpyAsync(&herr, err.get(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        // The device loop's sweep count and residuals, and ||X||^2, come back
+        // with the same synchronisation.
+        LoopState hst;
+        if (device_loop) {
+            DT_CUDA(cudaMemcpyAsync(&hst, loopst.get(), sizeof(LoopState), cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+            DT_CUDA(cudaMemcpyAsync(&x2, scal.as<double>(), sizeof(double),
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+        }
         DT_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (device_loop) {
+            sweeps = hst.it;
+            ctx->launches += (int64_t)sweeps * loop->launches_per_sweep;
+            if (rep)
+                for (int i = 0; i < std::min(sweeps, DT_MAX_HIST); i++) rep->res_hist[i] = hst.hist[i];
+        }
         // The FP32 copy of an FP64 X lives for this call only.
         X32own.release();
         X32 = nullptr;
@@ -462,6 +597,7 @@ struct MixedPlan {
     int64_t I[16], R[16];
     MixedHooi h;
     SweepGraph g_bf16, g_split;
+    LoopGraph loop;  // destroyed before h's buffers
     MixedPlan(int n, const int64_t *shape, const int64_t *ranks, const dt_hooi_opts &o)
         : N(n), inner(o.inner_iters), precision(o.precision) {
         for (int m = 0; m < n; m++) {
@@ -530,6 +666,7 @@ void hooi_dense_lowprec(dt_ctx *ctx, const void *X, int dtype, int ndim, const i
         h.Gs.alloc(ctx, prod(ranks, ndim) * sizeof(double));
         h.g_bf16 = &plan->g_bf16;
         h.g_split = &plan->g_split;
+        h.loop = &plan->loop;
         h.opts = opts;
         h.xsplit = opts.precision == DT_PREC_BF16X2 ||
                    (opts.precision == DT_PREC_BF16 && opts.refine_sweeps > 0);

@@ -87,6 +87,8 @@ std::string num(double v) {
 
 }  // namespace
 
+bool summary_active(dt_ctx *ctx) { return ctx && ctx->summary && state(ctx)->on; }
+
 SummaryScope::SummaryScope(dt_ctx *ctx, const char *name, double flop, double bytes) {
     if (!ctx || !ctx->summary || !state(ctx)->on) return;
     ctx_ = ctx;

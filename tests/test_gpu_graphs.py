@@ -2,9 +2,11 @@
 
 On a stream other than the legacy default stream, dt_hooi_dense keeps its
 buffers between calls with the same shapes and ranks and replays each sweep
-from a captured CUDA graph.  The results must equal direct launches (legacy
-stream, no graph) to FP64 rounding: the same kernels run in the same order.
-Tolerance: 1e-12 relative (norm-wise)."""
+from a captured CUDA graph; the tensor-core path's split sweeps run as one
+graph whose WHILE node repeats a sweep and its stop test on the device.  The
+results must equal direct launches (legacy stream, no graph, the host
+deciding after each sweep) to FP64 rounding: the same kernels run in the same
+order.  Tolerance: 1e-12 relative (norm-wise)."""
 import numpy as np
 import pytest
 
@@ -58,7 +60,10 @@ def test_graph_replay_matches_direct_launches(ctx, prec):
         assert r["precision_used"] == precision
         assert r["sweeps"] == r0["sweeps"]
         assert abs(r["residual"] - r0["residual"]) <= 1e-12
-        assert r["kernel_launches"] == r0["kernel_launches"]
+        # The split sweeps run as one device-side loop on a capturable stream:
+        # each sweep adds the loop's stop-test kernel.
+        extra = r["sweeps"] if precision == DT_PREC_BF16X2 else 0
+        assert r["kernel_launches"] == r0["kernel_launches"] + extra
         assert _nrel(G, G0) < 1e-12
         for n in range(3):
             assert _nrel(U[n], U0[n]) < 1e-12
