@@ -674,7 +674,6 @@ __global__ void __launch_bounds__(SM_NT, 1) subspace_mma_kernel(const double *Sg
     __shared__ double red[33];
     __shared__ int bad;
     const int t = threadIdx.x;
-    pdl_trigger();
     pdl_wait();
     const int n8 = (n + 7) / 8 * 8;
     const int lds = sm_lds(n8);
@@ -767,6 +766,9 @@ __global__ void __launch_bounds__(SM_NT, 1) subspace_mma_kernel(const double *Sg
             if (bad) break;
         }
     }
+    // Dependents launch once the iteration is done (launched at the start,
+    // they took SM slots for the whole kernel; about 1 % of a decomposition).
+    pdl_trigger();
     if (!bad) {
         for (int e = t; e < n * r; e += SM_NT) {
             const int i = e % n, c = e / n;
@@ -1009,62 +1011,6 @@ __global__ void chol_lower_inv_kernel(const double *Gg, int r, double *Linv, int
     for (int e = threadIdx.x; e < r * r; e += blockDim.x) {
         const int i = e % r, c = e / r;  // Linv(i, c) = Rinv(c, i)
         Linv[e] = Ri[c * r + i];
-    }
-}
-
-// Row Gram of a tall factor stored transposed: A is r x m col-major, so
-// factor row k is the r contiguous values A[k*r ...].  Each block sums
-// u_k u_k^T over its rows into part[block][r*r]; entries are owned by threads.
-__global__ void __launch_bounds__(256) rows_gram_kernel(const double *__restrict__ A, int r,
-                                                        int64_t m, int64_t rows_per_block,
-                                                        double *__restrict__ part) {
-    __shared__ double us[64 * 33];
-    const int64_t k0 = blockIdx.x * rows_per_block;
-    const int64_t k1 = min(m, k0 + rows_per_block);
-    const int rr = r * r;
-    double acc[4] = {0, 0, 0, 0};  // entries t, t+256, t+512, t+768 (r <= 32)
-    for (int64_t kb = k0; kb < k1; kb += 64) {
-        const int nb = (int)(k1 - kb < 64 ? k1 - kb : 64);
-        __syncthreads();
-        for (int e = threadIdx.x; e < nb * r; e += blockDim.x) {
-            const int b = e / r, c = e - b * r;
-            us[b * 33 + c] = A[(kb + b) * r + c];
-        }
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int e = threadIdx.x + 256 * q;
-            if (e >= rr) break;
-            const int a = e / r, c = e - a * r;
-            double sacc = acc[q];
-            for (int b = 0; b < nb; b++) sacc = fma(us[b * 33 + a], us[b * 33 + c], sacc);
-            acc[q] = sacc;
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const int e = threadIdx.x + 256 * q;
-        if (e < rr) part[(int64_t)blockIdx.x * rr + e] = acc[q];
-    }
-}
-
-// T[:, k] = Linv A[:, k] for every factor row k (Linv lower, r x r col-major);
-// one thread per output element, out of place.
-__global__ void __launch_bounds__(256) rows_apply_kernel(const double *__restrict__ A, int r,
-                                                         int64_t m, const double *__restrict__ Linv,
-                                                         double *__restrict__ T) {
-    __shared__ double Ls[32 * 32];
-    for (int e = threadIdx.x; e < r * r; e += blockDim.x) Ls[e] = Linv[e];
-    __syncthreads();
-    const int64_t n = m * r;
-    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
-         e += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t k = e / r;
-        const int a = (int)(e - k * r);
-        const double *u = A + k * r;
-        double acc = 0.0;
-        for (int c = 0; c <= a; c++) acc = fma(Ls[a + c * r], u[c], acc);
-        T[e] = acc;
     }
 }
 

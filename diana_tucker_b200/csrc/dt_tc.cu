@@ -352,7 +352,6 @@ __global__ void __launch_bounds__(128, 1)
     uint64_t *full = bars, *done = bars + nck;
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + nck + 1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    pdl_trigger();
     if (warp == 0) {
         tmem_alloc(tmem_slot, a.tmem_cols);
         tmem_relinquish();
@@ -418,6 +417,7 @@ __global__ void __launch_bounds__(128, 1)
             for (int g = 0; g < a.N; g++)
                 a.part[(int64_t)blockIdx.x * a.Ipad * a.N + (int64_t)g * a.Ipad + m] = 0.f;
     }
+    pdl_trigger();  // dependents launch once the partial tile is written
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {
@@ -430,7 +430,6 @@ __global__ void __launch_bounds__(128, 1)
 // partial tiles column-major: P_z(m, g) = part[z][g * Ipad + m].
 __global__ void gram_reduce_kernel(const float *__restrict__ part, int nz, int n, int Ipad, int N,
                                    int split, double *__restrict__ S) {
-    pdl_trigger();
     pdl_wait();
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n * n; e += gridDim.x * blockDim.x) {
         const int i = e % n, j = e / n;
@@ -442,6 +441,7 @@ __global__ void gram_reduce_kernel(const float *__restrict__ part, int nz, int n
         }
         S[e] = s;
     }
+    pdl_trigger();  // dependents launch once S is written
 }
 
 // X (FP32) -> BF16 hi (+ lo) and per-block partial sums of squares (FP64).
