@@ -149,7 +149,7 @@ __device__ bool warp_chol_inv(double *G, double *Rinv, int r) {
             if (lane >= i) g[i] = fma(-rki, g[k], g[i]);
         }
     }
-    if (!INV) {
+    if constexpr (!INV) {
         if (lane < r) {
 #pragma unroll
             for (int i = 0; i < RMAX; i++)
@@ -157,32 +157,33 @@ __device__ bool warp_chol_inv(double *G, double *Rinv, int r) {
         }
         __syncwarp();
         return ok;
-    }
-    // Column `lane` of R^{-1} by back substitution; x[j] = 0 for j > lane.
+    } else {
+        // Column `lane` of R^{-1} by back substitution; x[j] = 0 for j > lane.
 #pragma unroll
-    for (int i = 0; i < RMAX; i++) x[i] = (i == lane) ? invd[i] : 0.0;
+        for (int i = 0; i < RMAX; i++) x[i] = (i == lane) ? invd[i] : 0.0;
 #pragma unroll
-    for (int i = RMAX - 2; i >= 0; i--) {
-        if (i >= r - 1) continue;
-        double sacc = 0.0;
+        for (int i = RMAX - 2; i >= 0; i--) {
+            if (i >= r - 1) continue;
+            double sacc = 0.0;
 #pragma unroll
-        for (int j = i + 1; j < RMAX; j++) {
-            if (j >= r) break;
-            const double rij = __shfl_sync(0xffffffffu, g[i], j);
-            sacc = fma(rij, x[j], sacc);
-        }
-        if (i < lane) x[i] = -sacc * invd[i];
-    }
-    if (lane < r) {
-#pragma unroll
-        for (int i = 0; i < RMAX; i++)
-            if (i < r) {
-                Rinv[i * r + lane] = x[i];
-                G[i * r + lane] = i <= lane ? g[i] : 0.0;
+            for (int j = i + 1; j < RMAX; j++) {
+                if (j >= r) break;
+                const double rij = __shfl_sync(0xffffffffu, g[i], j);
+                sacc = fma(rij, x[j], sacc);
             }
+            if (i < lane) x[i] = -sacc * invd[i];
+        }
+        if (lane < r) {
+#pragma unroll
+            for (int i = 0; i < RMAX; i++)
+                if (i < r) {
+                    Rinv[i * r + lane] = x[i];
+                    G[i * r + lane] = i <= lane ? g[i] : 0.0;
+                }
+        }
+        __syncwarp();
+        return ok;
     }
-    __syncwarp();
-    return ok;
 }
 
 // Subspace iteration L <- orth(S L), `iters` times, one CTA.  S (n x n,
