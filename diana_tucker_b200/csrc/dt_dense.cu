@@ -35,6 +35,7 @@ __global__ void __launch_bounds__(TTM_NT) ttm_kernel(const TX *__restrict__ X, i
     __shared__ __align__(16) double Xs[TTM_BK][TTM_BP];
     __shared__ __align__(16) double Ms[TTM_BK][JT];
     const int t = threadIdx.x;
+    pdl_wait();
     const int64_t p0 = (int64_t)blockIdx.x * TTM_BP;
     const int64_t j0 = (int64_t)blockIdx.y * JT;
     const int64_t LI = L * I;
@@ -105,6 +106,7 @@ __global__ void __launch_bounds__(TTM_NT) ttm_kernel(const TX *__restrict__ X, i
         __syncthreads();
     }
 
+    pdl_trigger();  // dependents may launch while the outputs are stored
     const int64_t LJ = L * J;
 #pragma unroll
     for (int r = 0; r < 2; r++) {
@@ -159,6 +161,7 @@ __global__ void __launch_bounds__(TTM_NT) ttm_pipe_kernel(const TX *__restrict__
     auto Ms = reinterpret_cast<double(*)[TTM_BK][JT]>(pipe_smem);
     auto Xs = reinterpret_cast<TX(*)[XS_ELEMS]>(pipe_smem + 2 * TTM_BK * JT * sizeof(double));
     const int t = threadIdx.x;
+    pdl_wait();
     const int64_t p0 = (int64_t)blockIdx.x * TTM_BP;
     const int64_t j0 = (int64_t)blockIdx.y * JT;
     const int64_t ibeg = (int64_t)blockIdx.z * kchunk;
@@ -274,6 +277,7 @@ __global__ void __launch_bounds__(TTM_NT) ttm_pipe_kernel(const TX *__restrict__
         __syncthreads();
     }
 
+    pdl_trigger();  // dependents may launch while the outputs are stored
     const int64_t LJ = L * J;
 #pragma unroll
     for (int r = 0; r < 2; r++) {
@@ -319,6 +323,7 @@ __global__ void __launch_bounds__(TTM_NT) ttm_dmma_kernel(const TX *__restrict__
     auto Xs = reinterpret_cast<TX(*)[TTM_BK * TTM_DM_XROW]>(
         dm_smem + 2 * TTM_BK * TTM_DM_MROW * sizeof(double));
     const int t = threadIdx.x, w = t >> 5, lane = t & 31, g = lane >> 2, t4 = lane & 3;
+    pdl_wait();
     const int64_t p0 = (int64_t)blockIdx.x * TTM_BP;
     const int64_t j0 = (int64_t)blockIdx.y * 16;
     const int64_t ibeg = (int64_t)blockIdx.z * kchunk;
@@ -379,6 +384,7 @@ __global__ void __launch_bounds__(TTM_NT) ttm_dmma_kernel(const TX *__restrict__
         __syncthreads();
     }
 
+    pdl_trigger();  // dependents may launch while the outputs are stored
     // D[row g][col 2 t + h] of tile (m, n): row 64 w + 8 m + g, j = 8 n + 2 t + h.
     double *y = Y + l0 + L * J * b0;
 #pragma unroll
@@ -396,12 +402,14 @@ __global__ void __launch_bounds__(TTM_NT) ttm_dmma_kernel(const TX *__restrict__
 
 __global__ void sum_splits_kernel(const double *__restrict__ part, int nsplit, int64_t n,
                                   double *__restrict__ out) {
+    pdl_wait();
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
          e += (int64_t)gridDim.x * blockDim.x) {
         double s = 0.0;
         for (int z = 0; z < nsplit; z++) s += part[z * n + e];
         out[e] = s;
     }
+    pdl_trigger();
 }
 
 template <class TX, int JT>
@@ -434,19 +442,19 @@ void ttm_launch(dt_ctx *ctx, const TX *X, int64_t L, int64_t I, int64_t B, const
     auto launch = [&](double *dst) {
         if (JT == 16 && rows_ok) {
             smem_limit(ctx, ttm_dmma_kernel<TX>, smem_dmma);
-            DT_LAUNCH(ctx, ttm_dmma_kernel<TX>, grid, TTM_NT, smem_dmma, X, L, I, P, M, msj, msi,
+            DT_LAUNCH_PDL(ctx, ttm_dmma_kernel<TX>, grid, TTM_NT, smem_dmma, X, L, I, P, M, msj, msi,
                       J, dst, kchunk, ysize);
         } else if (rows_ok) {
             smem_limit(ctx, ttm_pipe_kernel<TX, JT, false>, smem_rows);
-            DT_LAUNCH(ctx, (ttm_pipe_kernel<TX, JT, false>), grid, TTM_NT, smem_rows, X, L, I, P,
+            DT_LAUNCH_PDL(ctx, (ttm_pipe_kernel<TX, JT, false>), grid, TTM_NT, smem_rows, X, L, I, P,
                       M, msj, msi, J, dst, kchunk, ysize);
         } else if (kfast_ok) {
             smem_limit(ctx, ttm_pipe_kernel<TX, JT, true>, smem_kfast);
-            DT_LAUNCH(ctx, (ttm_pipe_kernel<TX, JT, true>), grid, TTM_NT, smem_kfast, X, L, I, P,
+            DT_LAUNCH_PDL(ctx, (ttm_pipe_kernel<TX, JT, true>), grid, TTM_NT, smem_kfast, X, L, I, P,
                       M, msj, msi, J, dst, kchunk, ysize);
         }
         else
-            DT_LAUNCH(ctx, (ttm_kernel<TX, JT>), grid, TTM_NT, 0, X, L, I, P, M, msj, msi, J, dst,
+            DT_LAUNCH_PDL(ctx, (ttm_kernel<TX, JT>), grid, TTM_NT, 0, X, L, I, P, M, msj, msi, J, dst,
                       kchunk, ysize);
     };
     if (nsplit == 1) {
@@ -456,7 +464,7 @@ void ttm_launch(dt_ctx *ctx, const TX *X, int64_t L, int64_t I, int64_t B, const
     DevMem part(ctx, (size_t)nsplit * ysize * sizeof(double));
     launch(part.as<double>());
     const unsigned blocks = std::max(1u, std::min<unsigned>(ceil_div(ysize, 256), 8u * ctx->num_sms));
-    DT_LAUNCH(ctx, sum_splits_kernel, blocks, 256, 0, part.as<double>(), (int)nsplit, ysize, Y);
+    DT_LAUNCH_PDL(ctx, sum_splits_kernel, blocks, 256, 0, part.as<double>(), (int)nsplit, ysize, Y);
 }
 
 }  // namespace
@@ -742,12 +750,14 @@ namespace {
 template <class T>
 __global__ void sumsq_partial_kernel(const T *__restrict__ x, int64_t n,
                                      double *__restrict__ part) {
+    pdl_wait();
     double s = 0.0;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n;
          e += (int64_t)gridDim.x * blockDim.x) {
         const double v = (double)x[e];
         s = fma(v, v, s);
     }
+    pdl_trigger();
     __shared__ double red[32];
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
@@ -761,8 +771,10 @@ __global__ void sumsq_partial_kernel(const T *__restrict__ x, int64_t n,
 
 __global__ void sum_partials_kernel(const double *__restrict__ part, int n,
                                     double *__restrict__ out) {
+    pdl_wait();
     double s = 0.0;
     for (int e = threadIdx.x; e < n; e += blockDim.x) s += part[e];
+    pdl_trigger();
     __shared__ double red[32];
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
@@ -787,12 +799,12 @@ void sumsq(dt_ctx *ctx, const void *x, int dtype, int64_t n, double *out) {
     const int blocks = std::max(1, std::min<int>(4 * ctx->num_sms, (int)ceil_div(n, 256)));
     DevMem part(ctx, (size_t)blocks * sizeof(double));
     if (dtype == DT_F64)
-        DT_LAUNCH(ctx, sumsq_partial_kernel<double>, blocks, 256, 0,
+        DT_LAUNCH_PDL(ctx, sumsq_partial_kernel<double>, blocks, 256, 0,
                   static_cast<const double *>(x), n, part.as<double>());
     else
-        DT_LAUNCH(ctx, sumsq_partial_kernel<float>, blocks, 256, 0,
+        DT_LAUNCH_PDL(ctx, sumsq_partial_kernel<float>, blocks, 256, 0,
                   static_cast<const float *>(x), n, part.as<double>());
-    DT_LAUNCH(ctx, sum_partials_kernel, 1, 1024, 0, part.as<double>(), blocks, out);
+    DT_LAUNCH_PDL(ctx, sum_partials_kernel, 1, 1024, 0, part.as<double>(), blocks, out);
 }
 
 void f32_to_f64(dt_ctx *ctx, const float *x, int64_t n, double *y) {
