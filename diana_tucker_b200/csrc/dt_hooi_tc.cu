@@ -42,6 +42,7 @@ struct LoopState {
 // `thr`, or `max_sweeps` done), and the loop's condition for the next pass.
 __global__ void sweep_check_kernel(cudaGraphConditionalHandle h, const double *scal,
                                    LoopState *st, double thr, int max_sweeps) {
+    pdl_wait();
     const double x2 = scal[0], g2 = scal[1];
     const double res = sqrt(fmax(0.0, 1.0 - g2 / x2));
     const int it = st->it;
@@ -141,7 +142,7 @@ struct MixedHooi {
             if (ok) {
                 try {
                     sweep();
-                    DT_LAUNCH(ctx, sweep_check_kernel, 1, 1, 0, h,
+                    DT_LAUNCH_PDL(ctx, sweep_check_kernel, 1, 1, 0, h,
                               (const double *)scal.as<double>(), loopst.as<LoopState>(), thr,
                               max_sweeps);
                 } catch (...) {

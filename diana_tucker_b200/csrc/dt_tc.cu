@@ -448,6 +448,7 @@ __global__ void gram_reduce_kernel(const float *__restrict__ part, int nz, int n
 __global__ void split_f32_kernel(const float *__restrict__ x, int64_t n,
                                  __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo,
                                  double *__restrict__ part) {
+    pdl_wait();
     double s = 0.0;
     const int64_t n4 = n / 4;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n4;
@@ -474,6 +475,7 @@ __global__ void split_f32_kernel(const float *__restrict__ x, int64_t n,
         if (lo) lo[e] = l;
         s = fma((double)v, (double)v, s);
     }
+    pdl_trigger();
     __shared__ double red[32];
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
@@ -500,6 +502,7 @@ __global__ void __launch_bounds__(256) core_rows_kernel(const __nv_bfloat16 *__r
     extern __shared__ double Us[];  // I x RMAX, row i at Us + i * RMAX
     __shared__ double red[4][64];
     __shared__ double s2w[8];
+    pdl_wait();
     for (int64_t e = threadIdx.x; e < I * RMAX; e += blockDim.x) {
         const int64_t i = e / RMAX;
         const int r = (int)(e - i * RMAX);
@@ -521,6 +524,7 @@ __global__ void __launch_bounds__(256) core_rows_kernel(const __nv_bfloat16 *__r
             for (int r = 0; r < RMAX; r++) acc[r] = fma(y, u[r], acc[r]);
         }
     }
+    pdl_trigger();  // dependents may launch while the core is stored
     double s2 = 0.0;
 #pragma unroll
     for (int r = 0; r < RMAX; r++) {
@@ -542,8 +546,10 @@ __global__ void __launch_bounds__(256) core_rows_kernel(const __nv_bfloat16 *__r
 }
 
 __global__ void sum_double_kernel(const double *__restrict__ part, int n, double *__restrict__ out) {
+    pdl_wait();
     double s = 0.0;
     for (int e = threadIdx.x; e < n; e += blockDim.x) s += part[e];
+    pdl_trigger();
     __shared__ double red[32];
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
@@ -756,8 +762,8 @@ void split_f32(dt_ctx *ctx, const float *x, int64_t n, __nv_bfloat16 *hi, __nv_b
                double *sumsq_out) {
     const int blocks = std::max(1, std::min<int>(4 * ctx->num_sms, (int)ceil_div(n / 4 + 1, 256)));
     DevMem part(ctx, (size_t)blocks * sizeof(double));
-    DT_LAUNCH(ctx, split_f32_kernel, blocks, 256, 0, x, n, hi, lo, part.as<double>());
-    DT_LAUNCH(ctx, sum_double_kernel, 1, 1024, 0, part.as<double>(), blocks, sumsq_out);
+    DT_LAUNCH_PDL(ctx, split_f32_kernel, blocks, 256, 0, x, n, hi, lo, part.as<double>());
+    DT_LAUNCH_PDL(ctx, sum_double_kernel, 1, 1024, 0, part.as<double>(), blocks, sumsq_out);
 }
 
 void split_f32_chunks(dt_ctx *ctx, const ChunkedUpload &up, __nv_bfloat16 *hi,
@@ -769,11 +775,11 @@ void split_f32_chunks(dt_ctx *ctx, const ChunkedUpload &up, __nv_bfloat16 *hi,
     for (int c = 0; c < up.chunks; c++) {
         up.wait(ctx, c);
         const int64_t off = up.offset(c);
-        DT_LAUNCH(ctx, split_f32_kernel, bpc, 256, 0, dx + off, up.length(c), hi + off,
+        DT_LAUNCH_PDL(ctx, split_f32_kernel, bpc, 256, 0, dx + off, up.length(c), hi + off,
                   lo ? lo + off : nullptr, part.as<double>() + (size_t)c * bpc);
     }
     // Partials in chunk order: the same sum on every call.
-    DT_LAUNCH(ctx, sum_double_kernel, 1, 1024, 0, part.as<double>(), up.chunks * bpc, sumsq_out);
+    DT_LAUNCH_PDL(ctx, sum_double_kernel, 1, 1024, 0, part.as<double>(), up.chunks * bpc, sumsq_out);
 }
 
 size_t core_rows_scratch_bytes(int64_t K) {
@@ -791,7 +797,7 @@ void core_rows(dt_ctx *ctx, const __nv_bfloat16 *Yh, const __nv_bfloat16 *Yl, in
     do {                                                                                     \
         const size_t smem = (size_t)I * RM * sizeof(double);                                 \
         smem_limit(ctx, core_rows_kernel<RM>, smem);                                         \
-        DT_LAUNCH(ctx, core_rows_kernel<RM>, blocks, 256, smem, Yh, Yl, I, K, U, (int)R, G,  \
+        DT_LAUNCH_PDL(ctx, core_rows_kernel<RM>, blocks, 256, smem, Yh, Yl, I, K, U, (int)R, G,  \
                   part);                                                                     \
     } while (0)
     if (R <= 8)
@@ -801,7 +807,7 @@ void core_rows(dt_ctx *ctx, const __nv_bfloat16 *Yh, const __nv_bfloat16 *Yl, in
     else
         DT_CORE_ROWS(32);
 #undef DT_CORE_ROWS
-    DT_LAUNCH(ctx, sum_double_kernel, 1, 1024, 0, part, blocks, g2_out);
+    DT_LAUNCH_PDL(ctx, sum_double_kernel, 1, 1024, 0, part, blocks, g2_out);
 }
 
 }  // namespace dt
