@@ -114,6 +114,7 @@ _SIGS = [
     ("dt_ctx_mem_usage", ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_uint64),
                                         ctypes.POINTER(ctypes.c_uint64)]),
     ("dt_selftest_wait_timeout", ctypes.c_int, [_vp, ctypes.c_int64]),
+    ("dt_libc_rand_sequence", ctypes.c_int, [ctypes.c_uint, ctypes.c_int64, _vp]),
     ("dt_ttm_f64", ctypes.c_int, [_vp, _vp, ctypes.c_int, c_i64p, ctypes.c_int, _vp,
                                   ctypes.c_int64, _vp]),
     ("dt_gram_f64", ctypes.c_int, [_vp, _vp, ctypes.c_int, c_i64p, ctypes.c_int, _vp]),

@@ -22,13 +22,51 @@ namespace dt {
 
 namespace {
 
-// Marsaglia polar draw on libc rand() -- the generator the reference's
-// Util::randn (src/util.cpp:10-18) uses for HOOI's initial factors, kept
-// identical so DT_INIT_RANDN_LIBC starts from the reference's factors.
-double libc_polar_randn() {
+}  // namespace
+
+// The sequence rand() returns after srand(seed) in the GNU C library, which
+// the reference's Util::randn draws from: its additive lagged-Fibonacci
+// generator of degree 31 and separation 3 (random(3), TYPE_3), restated.  The
+// 31-word state is filled by the Lehmer generator x <- 16807 x mod (2^31 - 1)
+// from the seed (0 taken as 1); each step adds the word 31 back to the word 3
+// back (mod 2^32) and returns the sum without its lowest bit; the first 310
+// steps are discarded.  Used for an explicit seed, it gives the library's own
+// draws without touching the process's rand() state.
+LibcRand::LibcRand(unsigned seed) {
+    int32_t word = (int32_t)(seed ? seed : 1u);
+    s_[0] = word;
+    for (int i = 1; i < 31; i++) {
+        const int64_t hi = word / 127773, lo = word % 127773;
+        int64_t w = 16807 * lo - 2836 * hi;
+        if (w < 0) w += 2147483647;
+        word = (int32_t)w;
+        s_[i] = word;
+    }
+    f_ = 3;
+    r_ = 0;
+    for (int i = 0; i < 310; i++) next();
+}
+
+int32_t LibcRand::next() {
+    const uint32_t v = (uint32_t)s_[f_] + (uint32_t)s_[r_];
+    s_[f_] = (int32_t)v;
+    f_ = f_ == 30 ? 0 : f_ + 1;
+    r_ = r_ == 30 ? 0 : r_ + 1;
+    return (int32_t)(v >> 1);
+}
+
+namespace {
+
+// Marsaglia polar draw on a rand()-like source -- the method of the
+// reference's Util::randn (src/util.cpp:10-18), kept identical so
+// DT_INIT_RANDN_LIBC starts from the reference's factors.  `gen` is the
+// library's restatement of the C library's generator (explicit seed) or
+// null for the process's own rand() (DT_SEED_KEEP).
+double libc_polar_randn(LibcRand *gen) {
+    constexpr double kRandMax = 2147483647.0;  // RAND_MAX of the GNU C library
     for (;;) {
-        const double u = ((double)rand() / (RAND_MAX)) * 2 - 1;
-        const double v = ((double)rand() / (RAND_MAX)) * 2 - 1;
+        const double u = ((double)(gen ? gen->next() : rand()) / kRandMax) * 2 - 1;
+        const double v = ((double)(gen ? gen->next() : rand()) / kRandMax) * 2 - 1;
         const double r = u * u + v * v;
         if (r == 0 || r > 1) continue;
         return u * std::sqrt(-2 * std::log(r) / r);
@@ -191,15 +229,28 @@ void DenseHooi::init_factors(double *const *U_user) {
     }
     if (opts.init == DT_INIT_RANDN_LIBC) {
         // hooi_als.tpp:74-81: U_rand(I_n x R_n).randn(); U_n = Q of reduced_QR.
-        if (opts.seed != DT_SEED_KEEP) srand(opts.seed);
+        int64_t total = 0;
+        for (int m = 0; m < N; m++) total += I[m] * R[m];
+        const bool seeded = opts.seed != DT_SEED_KEEP;
+        if (seeded && init_cached && init_seed == opts.seed) {
+            // The same seed draws the same factors: copy the orthonormal ones
+            // kept from the first call (the draws take ~0.1-0.5 ms of host time).
+            int64_t off = 0;
+            for (int m = 0; m < N; m++) {
+                DT_CUDA(cudaMemcpyAsync(U[m].get(), init_cache.as<double>() + off,
+                                        I[m] * R[m] * sizeof(double), cudaMemcpyDeviceToDevice,
+                                        ctx->stream));
+                off += I[m] * R[m];
+            }
+            return;
+        }
         // Draw every block in mode order (the reference's order), upload once,
         // then one batched orthonormalisation launch for all modes (any
         // orthonormal basis of span(U_rand) gives the same sweeps: the TTM
         // chain's Gram matrices only see U U^T).
-        int64_t total = 0;
-        for (int m = 0; m < N; m++) total += I[m] * R[m];
+        LibcRand gen(seeded ? opts.seed : 1u);
         std::vector<double> h((size_t)total);
-        for (auto &v : h) v = libc_polar_randn();
+        for (auto &v : h) v = libc_polar_randn(seeded ? &gen : nullptr);
         DevMem a(ctx, total * sizeof(double));
         DT_CUDA(cudaMemcpyAsync(a.get(), h.data(), total * sizeof(double), cudaMemcpyHostToDevice,
                                 ctx->stream));
@@ -212,6 +263,18 @@ void DenseHooi::init_factors(double *const *U_user) {
             off += I[m] * R[m];
         }
         orth_batch(ctx, N, ap.data(), qp.data(), I, R);
+        if (seeded) {
+            if (!init_cache.get()) init_cache.alloc(ctx, total * sizeof(double));
+            off = 0;
+            for (int m = 0; m < N; m++) {
+                DT_CUDA(cudaMemcpyAsync(init_cache.as<double>() + off, U[m].get(),
+                                        I[m] * R[m] * sizeof(double), cudaMemcpyDeviceToDevice,
+                                        ctx->stream));
+                off += I[m] * R[m];
+            }
+            init_cached = true;
+            init_seed = opts.seed;
+        }
         return;
     }
     // HOSVD: leading R_n eigenvectors of X_(n) X_(n)^T by subspace iteration
@@ -382,6 +445,14 @@ struct Fp64Plan {
 using namespace dt;
 
 extern "C" {
+
+int dt_libc_rand_sequence(unsigned seed, int64_t n, int32_t *out) {
+    return guard([&] {
+        DT_CHECK_ARG(n >= 0 && (n == 0 || out), "dt_libc_rand_sequence: bad arguments");
+        LibcRand g(seed);
+        for (int64_t i = 0; i < n; i++) out[i] = g.next();
+    });
+}
 
 void dt_hooi_default_opts(dt_hooi_opts *o) {
     if (!o) return;

@@ -10,6 +10,17 @@ namespace dt {
 
 // The FP64 HOOI: CUDA-core TTM chain over a dimension tree, FP64 Gram and
 // subspace iteration.  X may be FP64 or FP32 (read as FP32, computed in FP64).
+// The GNU C library's rand() sequence after srand(seed), restated (dt_hooi.cu).
+class LibcRand {
+   public:
+    explicit LibcRand(unsigned seed);
+    int32_t next();  // in [0, 2^31 - 1], as rand()
+
+   private:
+    int32_t s_[31];
+    int f_ = 3, r_ = 0;
+};
+
 struct DenseHooi {
     dt_ctx *ctx = nullptr;
     int dtype = DT_F64;
@@ -22,6 +33,10 @@ struct DenseHooi {
     std::vector<DevMem> U;    // I_n x R_n col-major
     DevMem S, work, flag, scal, G;
     bool allocated = false;
+    // Orthonormal initial factors of the last explicit seed (DT_INIT_RANDN_LIBC).
+    DevMem init_cache;
+    bool init_cached = false;
+    unsigned init_seed = 0;
     int hosvd_iters = 30;
     LaunchTimer *xtimer = nullptr;  // times the TTM launches that read X
 

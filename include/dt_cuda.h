@@ -67,9 +67,13 @@ typedef struct dt_ctx dt_ctx;
 
 typedef struct {
     int init;           /* DT_INIT_* */
-    unsigned seed;      /* for DT_INIT_RANDN_LIBC: srand(seed) first; DT_SEED_KEEP
-                           continues the process's current rand() sequence, as
-                           the reference's HOOI_ALS does after the caller's srand */
+    unsigned seed;      /* for DT_INIT_RANDN_LIBC: the draws of srand(seed)
+                           followed by rand() (the library's restatement of the
+                           C library's generator: the process's rand() state is
+                           left alone, and a context reuses the factors of a
+                           seed it has drawn); DT_SEED_KEEP continues the
+                           process's current rand() sequence, as the
+                           reference's HOOI_ALS does after the caller's srand */
     int max_sweeps;     /* reference: max_iter */
     double tol;         /* stop when |res_k - res_{k-1}| < tol; <= 0 runs max_sweeps */
     int inner_iters;    /* subspace iterations per mode (reference ALS_: 5) */
@@ -246,6 +250,11 @@ DT_API int dt_hooi_dense(dt_ctx *ctx, const void *X, int dtype, int ndim, const 
 /* Fills opts with the reference's behaviour: random libc init, 5 inner
  * iterations, FP64, no tolerance. */
 DT_API void dt_hooi_default_opts(dt_hooi_opts *opts);
+/* The first n values rand() returns after srand(seed) in the GNU C library, as
+ * the library's own restatement of that generator computes them: the draws of
+ * DT_INIT_RANDN_LIBC with an explicit seed, which leave the process's rand()
+ * state untouched.  No device needed; for checking against the C library. */
+DT_API int dt_libc_rand_sequence(unsigned seed, int64_t n, int32_t *out);
 
 /* ---- batched dense HOOI ------------------------------------------------ */
 typedef struct {

@@ -58,3 +58,21 @@ def test_null_arguments_are_rejected_without_a_device(lib):
     rc = lib.dt_ttm_f64(None, None, 3, None, 0, None, 1, None)
     assert rc == 1
     assert "dt_ctx" in lib.dt_last_error().decode()
+
+
+@pytest.mark.parametrize("seed", [1, 2, 5, 20000905, 0, 2**31 + 7, 2**32 - 2])
+def test_libc_rand_restatement_matches_the_c_library(lib, seed):
+    """DT_INIT_RANDN_LIBC with an explicit seed draws from the library's own
+    restatement of the C library's rand(); its sequence equals srand(seed)
+    followed by rand() (the reference's Util::randn source), value for value."""
+    import ctypes
+    import numpy as np
+    libc = ctypes.CDLL(None)
+    libc.rand.restype = ctypes.c_int
+    libc.srand.argtypes = [ctypes.c_uint]
+    n = 5000
+    out = np.zeros(n, dtype=np.int32)
+    assert lib.dt_libc_rand_sequence(seed, n, out.ctypes.data) == 0
+    libc.srand(seed)
+    ref = np.array([libc.rand() for _ in range(n)], dtype=np.int32)
+    assert np.array_equal(out, ref)
