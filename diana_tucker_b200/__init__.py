@@ -310,13 +310,19 @@ class Context:
         if on_device:
             import torch
             dev = X.device
-            # Column-major buffers: allocate the reversed shape row-major and
-            # permute back.
+            # One allocation for the core and the factors; each is a
+            # column-major view (the reversed shape row-major, permuted back).
             # Every entry is written by the library: no fill needed.
-            G = (torch.empty(ranks[::-1], dtype=torch.float64, device=dev)
-                 .permute(*range(N - 1, -1, -1)) if want_core else None)
-            U = ([torch.empty((ranks[n], shape[n]), dtype=torch.float64, device=dev).t()
-                  for n in range(N)] if (want_factors or U0 is not None) else None)
+            want_u = want_factors or U0 is not None
+            gsize = int(np.prod(ranks)) if want_core else 0
+            usizes = [shape[n] * ranks[n] for n in range(N)] if want_u else []
+            buf = torch.empty(gsize + sum(usizes), dtype=torch.float64, device=dev)
+            G = (buf[:gsize].view(ranks[::-1]).permute(*range(N - 1, -1, -1))
+                 if want_core else None)
+            U, off = ([] if want_u else None), gsize
+            for n, sz in enumerate(usizes):
+                U.append(buf[off:off + sz].view(ranks[n], shape[n]).t())
+                off += sz
             if U0 is not None:
                 for n in range(N):
                     U[n].copy_(torch.as_tensor(np.asarray(U0[n], dtype=np.float64)))

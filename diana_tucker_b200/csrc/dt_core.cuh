@@ -38,6 +38,11 @@ struct dt_ctx {
     static constexpr int kCopyChunks = 4;
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t copy_ev[kCopyChunks + 1] = {};
+    // Pinned host memory for the small read-backs (norms, residuals, error
+    // words): copies into it stay asynchronous, so a call queues all of them
+    // and synchronises once (allocated on first use).
+    static constexpr size_t kHostStageBytes = 4096;
+    void *host_stage = nullptr;
     // The dense HOOI drivers' last plans (device buffers plus a captured graph
     // of one sweep), reused by the next call with the same shapes, ranks and
     // options; released before the stream at dt_ctx_destroy.
@@ -262,6 +267,17 @@ struct ChunkedUpload {
 // device (the direction from unified addressing), on ctx->stream; the caller
 // synchronises once after its last copy.
 void copy_out(dt_ctx *ctx, void *user, const void *src, size_t bytes);
+
+// Queues n block copies on ctx->stream: one kernel launch when every
+// destination is device memory and every address and size is a multiple of
+// 8 bytes, else one copy_out per block.  Null destinations are skipped; at
+// most kMaxCopyBlocks blocks.
+constexpr int kMaxCopyBlocks = 17;
+void copy_blocks(dt_ctx *ctx, int n, void *const *dst, const void *const *src,
+                 const size_t *bytes);
+
+// The context's pinned read-back block (dt_ctx::kHostStageBytes bytes).
+void *host_stage(dt_ctx *ctx);
 
 // A caller buffer seen from the device: device pointers pass through, host
 // pointers are staged (copied in for inputs, copied back by finish() for

@@ -224,6 +224,76 @@ void copy_out(dt_ctx *ctx, void *user, const void *src, size_t bytes) {
     DT_CUDA(cudaMemcpyAsync(user, src, bytes, cudaMemcpyDefault, ctx->stream));
 }
 
+namespace {
+
+struct BlockList {
+    const unsigned long long *src[kMaxCopyBlocks];
+    unsigned long long *dst[kMaxCopyBlocks];
+    long long words[kMaxCopyBlocks];
+    int count;
+};
+
+// Every block in one grid-stride pass: 8-byte words, consecutive threads on
+// consecutive words.
+__global__ void copy_blocks_kernel(BlockList b) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int k = 0; k < b.count; k++)
+        for (long long i = t; i < b.words[k]; i += stride) b.dst[k][i] = b.src[k][i];
+}
+
+// Device (or managed) memory of the context's own GPU: a kernel there may
+// store to it without peer access.
+bool is_local_device_ptr(const dt_ctx *ctx, const void *p) {
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged) &&
+           attr.device == ctx->device;
+}
+
+}  // namespace
+
+void copy_blocks(dt_ctx *ctx, int n, void *const *dst, const void *const *src,
+                 const size_t *bytes) {
+    DT_CHECK_ARG(n >= 0 && n <= kMaxCopyBlocks, "copy_blocks: %d blocks", n);
+    BlockList b{};
+    bool one_launch = true;
+    long long most = 0;
+    for (int k = 0; k < n; k++) {
+        if (!dst[k] || bytes[k] == 0) continue;
+        const bool aligned = (reinterpret_cast<uintptr_t>(dst[k]) | reinterpret_cast<uintptr_t>(src[k]) |
+                              bytes[k]) % 8 == 0;
+        if (!aligned || !is_local_device_ptr(ctx, dst[k])) {
+            one_launch = false;
+            break;
+        }
+        b.src[b.count] = static_cast<const unsigned long long *>(src[k]);
+        b.dst[b.count] = static_cast<unsigned long long *>(dst[k]);
+        b.words[b.count] = (long long)(bytes[k] / 8);
+        most = std::max(most, b.words[b.count]);
+        b.count++;
+    }
+    if (!one_launch) {
+        for (int k = 0; k < n; k++)
+            if (dst[k]) copy_out(ctx, dst[k], src[k], bytes[k]);
+        return;
+    }
+    if (b.count == 0) return;
+    const int threads = 256;
+    const long long want = (most + threads - 1) / threads;
+    const unsigned blocks = (unsigned)std::max(1LL, std::min<long long>(want, 2LL * ctx->num_sms));
+    DT_LAUNCH(ctx, copy_blocks_kernel, blocks, threads, 0, b);
+}
+
+void *host_stage(dt_ctx *ctx) {
+    if (!ctx->host_stage)
+        DT_CUDA(cudaHostAlloc(&ctx->host_stage, dt_ctx::kHostStageBytes, cudaHostAllocDefault));
+    return ctx->host_stage;
+}
+
 void DevView::finish() {
     if (output_ && staged_ && bytes_) {
         DT_CUDA(cudaMemcpyAsync(user_, dptr_, bytes_, cudaMemcpyDeviceToHost, ctx_->stream));
@@ -291,6 +361,7 @@ int dt_ctx_destroy(dt_ctx *ctx) {
             cudaStreamDestroy(ctx->copy_stream);
         }
         if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+        if (ctx->host_stage) cudaFreeHost(ctx->host_stage);
         delete ctx;
     });
 }

@@ -216,13 +216,14 @@ void DenseHooi::sweep() {
     node(0, N, Xdev, dtype, shape);
 }
 
-void DenseHooi::init_factors(double *const *U_user) {
+void DenseHooi::init_factors(double *const *U_user, double *const *dst) {
+    auto out = [&](int m) { return dst ? dst[m] : U[m].as<double>(); };
     if (opts.init == DT_INIT_GIVEN) {
         DT_CHECK_ARG(U_user, "DT_INIT_GIVEN needs initial factors in U");
         for (int m = 0; m < N; m++) {
             DT_CHECK_ARG(U_user[m], "DT_INIT_GIVEN: U[%d] is NULL", m);
             DevView u(ctx, U_user[m], I[m] * R[m] * sizeof(double), true, false);
-            DT_CUDA(cudaMemcpyAsync(U[m].get(), u.ptr(), I[m] * R[m] * sizeof(double),
+            DT_CUDA(cudaMemcpyAsync(out(m), u.ptr(), I[m] * R[m] * sizeof(double),
                                     cudaMemcpyDeviceToDevice, ctx->stream));
         }
         return;
@@ -234,14 +235,19 @@ void DenseHooi::init_factors(double *const *U_user) {
         const bool seeded = opts.seed != DT_SEED_KEEP;
         if (seeded && init_cached && init_seed == opts.seed) {
             // The same seed draws the same factors: copy the orthonormal ones
-            // kept from the first call (the draws take ~0.1-0.5 ms of host time).
+            // kept from the first call (the draws take ~0.1-0.5 ms of host time),
+            // all modes in one launch.
+            void *d[16];
+            const void *src[16];
+            size_t bytes[16];
             int64_t off = 0;
             for (int m = 0; m < N; m++) {
-                DT_CUDA(cudaMemcpyAsync(U[m].get(), init_cache.as<double>() + off,
-                                        I[m] * R[m] * sizeof(double), cudaMemcpyDeviceToDevice,
-                                        ctx->stream));
+                d[m] = out(m);
+                src[m] = init_cache.as<double>() + off;
+                bytes[m] = I[m] * R[m] * sizeof(double);
                 off += I[m] * R[m];
             }
+            copy_blocks(ctx, N, d, src, bytes);
             return;
         }
         // Draw every block in mode order (the reference's order), upload once,
@@ -259,7 +265,7 @@ void DenseHooi::init_factors(double *const *U_user) {
         int64_t off = 0;
         for (int m = 0; m < N; m++) {
             ap[m] = a.as<double>() + off;
-            qp[m] = U[m].as<double>();
+            qp[m] = out(m);
             off += I[m] * R[m];
         }
         orth_batch(ctx, N, ap.data(), qp.data(), I, R);
@@ -267,7 +273,7 @@ void DenseHooi::init_factors(double *const *U_user) {
             if (!init_cache.get()) init_cache.alloc(ctx, total * sizeof(double));
             off = 0;
             for (int m = 0; m < N; m++) {
-                DT_CUDA(cudaMemcpyAsync(init_cache.as<double>() + off, U[m].get(),
+                DT_CUDA(cudaMemcpyAsync(init_cache.as<double>() + off, out(m),
                                         I[m] * R[m] * sizeof(double), cudaMemcpyDeviceToDevice,
                                         ctx->stream));
                 off += I[m] * R[m];
@@ -297,6 +303,9 @@ void DenseHooi::init_factors(double *const *U_user) {
         subspace_iter(ctx, S.as<double>(), I[m], U[m].as<double>(), R[m], hosvd_iters,
                       work.as<double>(), flag.as<int>());
         DT_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (dst)
+            DT_CUDA(cudaMemcpyAsync(dst[m], U[m].get(), I[m] * R[m] * sizeof(double),
+                                    cudaMemcpyDeviceToDevice, ctx->stream));
     }
 }
 
@@ -319,17 +328,19 @@ double DenseHooi::x_pass_bytes() const {
     return 2.0 * xsize * (dtype == DT_F64 ? 8 : 4);
 }
 
+// Through the context's pinned block: an asynchronous copy and one
+// synchronisation.
 void DenseHooi::read_scalars(int k, int n, double *out) {
-    DT_CUDA(cudaMemcpyAsync(out, scal.as<double>() + k, n * sizeof(double),
+    double *st = static_cast<double *>(host_stage(ctx));
+    DT_CUDA(cudaMemcpyAsync(st, scal.as<double>() + k, n * sizeof(double),
                             cudaMemcpyDeviceToHost, ctx->stream));
     DT_CUDA(cudaStreamSynchronize(ctx->stream));
+    std::memcpy(out, st, n * sizeof(double));
 }
 
 double DenseHooi::read_scalar(int k) {
     double h = 0.0;
-    DT_CUDA(cudaMemcpyAsync(&h, scal.as<double>() + k, sizeof(double), cudaMemcpyDeviceToHost,
-                            ctx->stream));
-    DT_CUDA(cudaStreamSynchronize(ctx->stream));
+    read_scalars(k, 1, &h);
     return h;
 }
 
@@ -386,20 +397,26 @@ void DenseHooi::run(double *G_user, double *const *U_user, dt_hooi_report *rep,
         sumsq(ctx, G.get(), DT_F64, prod(R, N), scal.as<double>() + 1);
     }
     DT_CUDA(cudaEventRecord(ctx->ev_stop, ctx->stream));
+    // The outputs go straight from the plan's buffers into the caller's (host
+    // or device), queued with the read-back of ||G||^2: one synchronisation.
+    {
+        void *dst[kMaxCopyBlocks];
+        const void *src[kMaxCopyBlocks];
+        size_t bytes[kMaxCopyBlocks];
+        dst[0] = G_user;
+        src[0] = G.get();
+        bytes[0] = prod(R, N) * sizeof(double);
+        for (int m = 0; m < N; m++) {
+            dst[1 + m] = U_user ? U_user[m] : nullptr;
+            src[1 + m] = U[m].get();
+            bytes[1 + m] = I[m] * R[m] * sizeof(double);
+        }
+        copy_blocks(ctx, 1 + N, dst, src, bytes);
+    }
     const double g2 = read_scalar(1);
-    int fl = 0;
-    DT_CUDA(cudaMemcpyAsync(&fl, flag.get(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-    DT_CUDA(cudaStreamSynchronize(ctx->stream));
     float ms = 0.f;
     DT_CUDA(cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop));
     if (!std::isfinite(g2)) fail(DT_ERR_NUMERIC, "HOOI produced a non-finite core");
-    // Straight from the plan's buffers into the caller's (host or device),
-    // one synchronisation for all.
-    if (G_user) copy_out(ctx, G_user, G.get(), prod(R, N) * sizeof(double));
-    if (U_user)
-        for (int m = 0; m < N; m++)
-            if (U_user[m]) copy_out(ctx, U_user[m], U[m].get(), I[m] * R[m] * sizeof(double));
-    DT_CUDA(cudaStreamSynchronize(ctx->stream));
     if (rep) {
         rep->sweeps = sweeps;
         rep->x_norm = std::sqrt(x2);

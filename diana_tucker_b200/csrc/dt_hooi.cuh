@@ -45,7 +45,9 @@ struct DenseHooi {
     // stays valid.
     void setup(dt_ctx *c, const void *X, int dtype, int n, const int64_t *shape,
                const int64_t *ranks, const dt_hooi_opts &o);
-    void init_factors(double *const *U_user);
+    // Writes the initial factors into dst[m] (I_m x R_m col-major device
+    // buffers; null: this object's U).
+    void init_factors(double *const *U_user, double *const *dst = nullptr);
     // graph: replays the sweep from a captured CUDA graph (null: launch
     // directly; never used with opts.profile).
     void run(double *G_user, double *const *U_user, dt_hooi_report *rep,

@@ -371,17 +371,19 @@ struct MixedHooi {
         return 2.0 * xsize * (R[N - 1] + R[mid - 1]);
     }
 
+    // Through the context's pinned block: an asynchronous copy and one
+    // synchronisation.
     void read_scalars(int k, int n, double *out) {
-        DT_CUDA(cudaMemcpyAsync(out, scal.as<double>() + k, n * sizeof(double),
+        double *st = static_cast<double *>(host_stage(ctx));
+        DT_CUDA(cudaMemcpyAsync(st, scal.as<double>() + k, n * sizeof(double),
                                 cudaMemcpyDeviceToHost, ctx->stream));
         DT_CUDA(cudaStreamSynchronize(ctx->stream));
+        std::memcpy(out, st, n * sizeof(double));
     }
 
     double read_scalar(int k) {
         double h = 0.0;
-        DT_CUDA(cudaMemcpyAsync(&h, scal.as<double>() + k, sizeof(double), cudaMemcpyDeviceToHost,
-                                ctx->stream));
-        DT_CUDA(cudaStreamSynchronize(ctx->stream));
+        read_scalars(k, 1, &h);
         return h;
     }
 
@@ -421,10 +423,11 @@ struct MixedHooi {
                       dtype == DT_F32 ? scal.as<double>() : x2f.as<double>());
         // Initial factors: the FP64 driver's generators (libc Gaussian + QR,
         // or the caller's); HOSVD is not offered on this path.
-        helper.init_factors(U_user);
-        for (int m = 0; m < N; m++)
-            DT_CUDA(cudaMemcpyAsync(U[m].get(), helper.U[m].get(), I[m] * R[m] * sizeof(double),
-                                    cudaMemcpyDeviceToDevice, ctx->stream));
+        {
+            double *dst[16];
+            for (int m = 0; m < N; m++) dst[m] = U[m].as<double>();
+            helper.init_factors(U_user, dst);
+        }
         // ||X||^2 is read with the first sweep's ||G||^2 (one synchronisation).
         double x2 = -1.0;
         // Phases: BF16 sweeps until the residual settles to the BF16 noise
@@ -541,29 +544,43 @@ struct MixedHooi {
         const int gslot = 2;
         DT_CUDA(cudaEventRecord(ctx->ev_stop, ctx->stream));
         // The outputs are copied (host or device, straight from the plan's
-        // buffers) before the one synchronisation that reads ||G||^2 and the
-        // kernels' error word.
-        if (G_user) copy_out(ctx, G_user, gsrc, prod(R, N) * sizeof(double));
-        if (U_user)
-            for (int m = 0; m < N; m++)
-                if (U_user[m])
-                    copy_out(ctx, U_user[m], U[m].get(), I[m] * R[m] * sizeof(double));
-        double g2 = 0.0;
-        int herr = 0;
-        DT_CUDA(cudaMemcpyAsync(&g2, scal.as<double>() + gslot, sizeof(double),
-                                cudaMemcpyDeviceToHost, ctx->stream));
-        DT_CUDA(cudaMemcpyAsync(&herr, err.get(), sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-        // The device loop's sweep count and residuals, and ||X||^2, come back
-        // with the same synchronisation.
-        LoopState hst;
-        if (device_loop) {
-            DT_CUDA(cudaMemcpyAsync(&hst, loopst.get(), sizeof(LoopState), cudaMemcpyDeviceToHost,
-                                    ctx->stream));
-            DT_CUDA(cudaMemcpyAsync(&x2, scal.as<double>(), sizeof(double),
-                                    cudaMemcpyDeviceToHost, ctx->stream));
+        // buffers) before the one synchronisation that reads ||X||^2 and
+        // ||G||^2, the kernels' error word and the device loop's sweep count
+        // and residuals (all into the context's pinned block).
+        {
+            void *dst[kMaxCopyBlocks];
+            const void *src[kMaxCopyBlocks];
+            size_t bytes[kMaxCopyBlocks];
+            dst[0] = G_user;
+            src[0] = gsrc;
+            bytes[0] = prod(R, N) * sizeof(double);
+            for (int m = 0; m < N; m++) {
+                dst[1 + m] = U_user ? U_user[m] : nullptr;
+                src[1 + m] = U[m].get();
+                bytes[1 + m] = I[m] * R[m] * sizeof(double);
+            }
+            copy_blocks(ctx, 1 + N, dst, src, bytes);
         }
+        constexpr size_t kErrAt = 32, kLoopAt = 64;
+        static_assert(kLoopAt + sizeof(LoopState) <= dt_ctx::kHostStageBytes, "stage too small");
+        char *st = static_cast<char *>(host_stage(ctx));
+        DT_CUDA(cudaMemcpyAsync(st, scal.as<double>(), (gslot + 1) * sizeof(double),
+                                cudaMemcpyDeviceToHost, ctx->stream));
+        DT_CUDA(cudaMemcpyAsync(st + kErrAt, err.get(), sizeof(int), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+        if (device_loop)
+            DT_CUDA(cudaMemcpyAsync(st + kLoopAt, loopst.get(), sizeof(LoopState),
+                                    cudaMemcpyDeviceToHost, ctx->stream));
         DT_CUDA(cudaStreamSynchronize(ctx->stream));
+        double sc[gslot + 1];
+        std::memcpy(sc, st, sizeof(sc));
+        const double g2 = sc[gslot];
+        int herr = 0;
+        std::memcpy(&herr, st + kErrAt, sizeof(int));
         if (device_loop) {
+            LoopState hst;
+            std::memcpy(&hst, st + kLoopAt, sizeof(LoopState));
+            x2 = sc[0];
             sweeps = hst.it;
             ctx->launches += (int64_t)sweeps * loop->launches_per_sweep;
             if (rep)
