@@ -445,6 +445,12 @@ def run_ours(args):
                                "what": "X read as split hi+lo BF16 in every pass (4 B per "
                                        "element) instead of BF16 hi only (2 B)"},
         "decompositions_per_s": round(world * 1000.0 / ms, 3) if ms > 0 else None,
+        # Each timed call's own device time (library events from its first to
+        # its last kernel): `value` minus this is the host time between calls.
+        "device_ms_per_call": {
+            "median": round(float(np.median([r["device_ms"] for r in reps])), 4),
+            "min": round(float(min(r["device_ms"] for r in reps)), 4),
+            "max": round(float(max(r["device_ms"] for r in reps)), 4)} if reps else None,
         "e2e": {"value": round(e2e_ms, 4), "unit": "ms", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "h2d_bare_ms": round(h2d_ms, 4),
                 "h2d_bare_gbs": round(h2d / h2d_ms / 1e6, 1) if h2d_ms > 0 else None,
