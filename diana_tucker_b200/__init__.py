@@ -29,6 +29,26 @@ def _is_torch(x) -> bool:
     return type(x).__module__.startswith("torch")
 
 
+def _column_major_outputs(shape, ranks, want_core, want_factors, device):
+    """The core (ranks, column-major) and the factors (shape[n] x ranks[n],
+    column-major) as float64 views of one uninitialised torch allocation on
+    `device`, the core first, then U_0, U_1, ...  The library writes every
+    entry.  Returns (G or None, [U_n] or None)."""
+    import torch
+    N = len(shape)
+    gsize = int(np.prod(ranks)) if want_core else 0
+    usizes = [int(shape[n]) * int(ranks[n]) for n in range(N)] if want_factors else []
+    buf = torch.empty(gsize + sum(usizes), dtype=torch.float64, device=device)
+    # A column-major view: the reversed shape row-major, permuted back.
+    G = (buf[:gsize].view(list(ranks)[::-1]).permute(*range(N - 1, -1, -1))
+         if want_core else None)
+    U, off = ([] if want_factors else None), gsize
+    for n, sz in enumerate(usizes):
+        U.append(buf[off:off + sz].view(int(ranks[n]), int(shape[n])).t())
+        off += sz
+    return G, U
+
+
 def _shape_arr(shape):
     return np.ascontiguousarray(np.asarray(shape, dtype=np.int64))
 
@@ -309,20 +329,8 @@ class Context:
         on_device = bool(device_out and is_torch and X.is_cuda)
         if on_device:
             import torch
-            dev = X.device
-            # One allocation for the core and the factors; each is a
-            # column-major view (the reversed shape row-major, permuted back).
-            # Every entry is written by the library: no fill needed.
-            want_u = want_factors or U0 is not None
-            gsize = int(np.prod(ranks)) if want_core else 0
-            usizes = [shape[n] * ranks[n] for n in range(N)] if want_u else []
-            buf = torch.empty(gsize + sum(usizes), dtype=torch.float64, device=dev)
-            G = (buf[:gsize].view(ranks[::-1]).permute(*range(N - 1, -1, -1))
-                 if want_core else None)
-            U, off = ([] if want_u else None), gsize
-            for n, sz in enumerate(usizes):
-                U.append(buf[off:off + sz].view(ranks[n], shape[n]).t())
-                off += sz
+            G, U = _column_major_outputs(shape, ranks, want_core,
+                                         want_factors or U0 is not None, X.device)
             if U0 is not None:
                 for n in range(N):
                     U[n].copy_(torch.as_tensor(np.asarray(U0[n], dtype=np.float64)))
