@@ -12,6 +12,7 @@ The C++ drop-in for the reference's own API (``Tensor<Ty>``, ``SpTensor<Ty>``,
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 
 import numpy as np
@@ -35,16 +36,23 @@ def _column_major_outputs(shape, ranks, want_core, want_factors, device):
     `device`, the core first, then U_0, U_1, ...  The library writes every
     entry.  Returns (G or None, [U_n] or None)."""
     import torch
-    N = len(shape)
-    gsize = int(np.prod(ranks)) if want_core else 0
-    usizes = [int(shape[n]) * int(ranks[n]) for n in range(N)] if want_factors else []
+    shape = [int(i) for i in shape]
+    ranks = [int(r) for r in ranks]
+    gsize = math.prod(ranks) if want_core else 0
+    usizes = [i * r for i, r in zip(shape, ranks)] if want_factors else []
     buf = torch.empty(gsize + sum(usizes), dtype=torch.float64, device=device)
-    # A column-major view: the reversed shape row-major, permuted back.
-    G = (buf[:gsize].view(list(ranks)[::-1]).permute(*range(N - 1, -1, -1))
-         if want_core else None)
+    # One as_strided view each (a view op costs a few microseconds of host
+    # time per call): column-major strides 1, R_0, R_0 R_1, ...
+    G = None
+    if want_core:
+        strides, st = [], 1
+        for r in ranks:
+            strides.append(st)
+            st *= r
+        G = buf.as_strided(ranks, strides, 0)
     U, off = ([] if want_factors else None), gsize
-    for n, sz in enumerate(usizes):
-        U.append(buf[off:off + sz].view(int(ranks[n]), int(shape[n])).t())
+    for i, r, sz in zip(shape, ranks, usizes):
+        U.append(buf.as_strided((i, r), (1, i), off))
         off += sz
     return G, U
 
