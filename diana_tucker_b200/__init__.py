@@ -301,8 +301,9 @@ class Context:
                    device_out=False):
         """Algorithm::Tucker::HOOI_ALS.  X: numpy or torch (float64/float32),
         column-major.  Returns (G, U, report-dict); with device_out and a CUDA
-        torch X, G and U are float64 CUDA tensors with column-major strides
-        (no copy back to the host), else numpy arrays."""
+        torch X, G and U are float64 CUDA tensors with column-major strides,
+        views of one device allocation (no copy back to the host), else numpy
+        arrays."""
         self._bind(X)
         is_torch = _is_torch(X)
         if is_torch:
